@@ -1,0 +1,146 @@
+/*
+ * nlsb200 — C ABI of the B200-native Lanczos exponential integrators
+ * (nonlinear Klein-Gordon / stochastic phi^4 Gautschi and Stormer-Verlet,
+ * cubic NLSE Strang SS2 and SEWI) of konradha/nlsolvers-datagen.
+ *
+ * Plain pointers and sizes only. Every entry point returns an int status:
+ * NLS_OK (0) or a negative NLS_ERR_* code; nls_last_error() gives the message.
+ * Host arrays are C-order (nz, ny, nx) / (ny, nx) with x fastest, FP64
+ * ('<f8') or interleaved complex128 ('<c16'), exactly the .npy payloads the
+ * reference drivers read and write. Grid sizes include the ghost ring, as the
+ * drivers' argv (device/drivers/kg_driver_dev_2d.cpp:35-55).
+ *
+ * Ownership: the caller owns every host buffer; a handle/pool owns all of its
+ * device memory. A handle or pool is single-threaded; different handles may be
+ * used from different threads.
+ */
+#ifndef NLSB200_H
+#define NLSB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NLS_OK 0
+#define NLS_ERR_INVALID_ARG -1 /* bad sizes, k, method, null pointer */
+#define NLS_ERR_SHAPE -2       /* array shape does not match the grid */
+#define NLS_ERR_NO_MEMORY -3   /* device or pinned host allocation failed */
+#define NLS_ERR_CUDA -4        /* CUDA runtime / launch error */
+#define NLS_ERR_NO_DEVICE -5   /* no CUDA device */
+#define NLS_ERR_CAPACITY -6    /* pool has no free slot or memory for the request */
+#define NLS_ERR_STATE -7       /* call not valid in the current state */
+#define NLS_ERR_NUMERIC -8     /* eigensolver did not converge / non-finite state */
+#define NLS_ERR_IO -9          /* file or .npy format error (CLI helpers) */
+
+/* Integrators (device/drivers/CMakeLists.txt:15-31). */
+#define NLS_KG_GAUTSCHI 0  /* kg_gautschi_{2d,3d}_dev: KGESolverDevice::step (kg_dev.hpp:97) */
+#define NLS_KG_SV 1        /* kg_sv_{2d,3d}_dev: KGESolverDevice::step_sv (kg_dev.hpp:102) */
+#define NLS_SP4_SV 2       /* sp4_sv_{2d,3d}_dev: SP4SolverDevice::step (stochastic_phi4_dev.hpp) */
+#define NLS_SP4_GAUTSCHI 3 /* Gautschi step with the phi^4 force (extension) */
+#define NLS_NLSE_SS2 4     /* nlse_{2d,3d}_dev: NLSESolverDevice::step (nlse_dev.hpp:187) */
+#define NLS_NLSE_SEWI 5    /* nlse_sewi_{2d,3d}_dev: NLSESolverDevice::step_sewi (nlse_dev.hpp:205) */
+
+#define NLS_FP32 0 /* FP32 / complex64 Krylov basis, compensated FP32 fields */
+#define NLS_FP64 1 /* FP64 / complex128 throughout */
+
+/*
+ * Problem description. Replaces the positional argv of the drivers plus the
+ * solver Parameters structs (kg_dev.hpp:21-30, nlse_dev.hpp:68-76).
+ * Derived exactly as the drivers: dx = 2 Lx/(nx-1), dy = 2 Ly/(ny-1),
+ * dt = T/nt, freq = nt/ns; the operator scale is 1/(dx dy) in 2-D and
+ * 1/dx^2 in 3-D (laplacians.hpp:100, :215).
+ * Nonlinearity (KG / phi^4): g(u) = (p1 m + q1) u + (p3 m + q3) u^3 + (rm m + r0) xi
+ *   reference KG  (kg_single.cuh:106-109):   p3 = -1
+ *   reference phi4 (stochastic_phi4.cuh:52): p1 = -1, p3 = 1, rm = -0.01 sqrt(2 dx)/dt
+ * NLSE density rho = (p3 m + q3)|u|^2 (reference: p3 = 1).
+ * xi ~ N(0,1) per (seed, step, point) from Philox4x32-10 + Box-Muller.
+ */
+typedef struct nls_problem {
+  int32_t dim;          /* 2 or 3 */
+  int32_t nx, ny, nz;   /* grid incl. ghost ring; nz ignored in 2-D */
+  double Lx, Ly, Lz;
+  double T;
+  int32_t nt, ns;       /* steps (the loop runs i = 1..nt-1) and snapshots */
+  int32_t k;            /* Krylov dimension, 3..32 (Gautschi / NLSE) */
+  int32_t method;       /* NLS_KG_GAUTSCHI ... NLS_NLSE_SEWI */
+  int32_t precision;    /* NLS_FP32 or NLS_FP64 */
+  int32_t sewi_variant; /* 0: the reference's operand order, 1: corrected */
+  int32_t has_c;        /* 0: c == 1 (c pointer may be NULL) */
+  int32_t reserved;
+  double p1, q1, p3, q3, rm, r0;
+  uint64_t seed;
+} nls_problem;
+
+typedef struct nls_handle nls_handle;
+typedef struct nls_pool nls_pool;
+
+/* Fill *p with the reference driver's defaults for `method` (nonlinearity,
+   k per binary: KG/phi4 10, NLSE SS2 2-D 20 / 3-D 25, SEWI 2-D 10 / 3-D 15). */
+int nls_problem_defaults(nls_problem *p, int32_t method, int32_t dim);
+
+/* ---- single trajectory: replaces KGESolverDevice (kg_dev.hpp:32-131),
+   SP4SolverDevice (stochastic_phi4_dev.hpp:29-33) and NLSESolverDevice
+   (nlse_dev.hpp:78-335) together with the driver loop
+   (kg_driver_dev_2d.cpp:144-153, nlse_cubic_driver_2d.cpp:106-110). */
+
+/* u0: n doubles (NLSE: n complex128), v0: n doubles (KG/phi4; NULL = 0),
+   m, c: n doubles (c may be NULL when has_c = 0). Snapshot 0 is the input. */
+int nls_create(const nls_problem *p, const double *u0, const double *v0, const double *m,
+               const double *c, nls_handle **out);
+/* Advance by nsteps steps (step + ghost copies + snapshot cadence each). */
+int nls_step(nls_handle *h, int32_t nsteps);
+/* Run every remaining step of the driver loop (i up to nt-1). */
+int nls_run(nls_handle *h);
+/* Copy the ns snapshots (ns*n values) to host: traj (NLSE: complex128), vel
+   (KG/phi4 only, may be NULL). Waits for outstanding work. */
+int nls_snapshot(nls_handle *h, double *traj, double *vel);
+/* Steps completed so far. */
+int nls_steps_done(nls_handle *h, int32_t *steps);
+int nls_destroy(nls_handle *h);
+
+/* ---- batched pool with continuous batching: many trajectories of one
+   (method, dim, k, precision) but any grid sizes step together; requests are
+   admitted into free slots between steps while others keep running. */
+int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
+                    int64_t capacity_points, int32_t max_slots, nls_pool **out);
+/* Admit one trajectory. traj_dst (ns*n values) and vel_dst (KG/phi4, may be
+   NULL) receive the snapshots asynchronously; they must stay valid until the
+   slot is released. Returns NLS_ERR_CAPACITY when it does not fit now. */
+int nls_pool_admit(nls_pool *pool, const nls_problem *p, const double *u0, const double *v0,
+                   const double *m, const double *c, double *traj_dst, double *vel_dst,
+                   int32_t *slot_out);
+/* Advance every unfinished slot by up to nsteps steps. */
+int nls_pool_step(nls_pool *pool, int32_t nsteps);
+/* steps_done: completed steps; finished: 1 when all steps ran and every
+   snapshot has reached the host buffers. */
+int nls_pool_poll(nls_pool *pool, int32_t slot, int32_t *steps_done, int32_t *finished);
+/* Free the slot (waits for its outstanding snapshot copies). */
+int nls_pool_release(nls_pool *pool, int32_t slot);
+/* Wait for all queued device work and copies. */
+int nls_pool_sync(nls_pool *pool);
+/* Number of occupied slots, and free device points. */
+int nls_pool_usage(nls_pool *pool, int32_t *occupied, int64_t *free_points);
+/* 1: capture each step as a CUDA graph (default), 0: direct launches. */
+int nls_pool_set_graphs(nls_pool *pool, int32_t enable);
+/* Rows of the march segment (tile length along y in 2-D / z in 3-D). */
+int nls_pool_set_segment(nls_pool *pool, int32_t rows);
+/* Time `iters` launches of Lanczos pass j (1 <= j <= k-2) on the current state
+   with CUDA events; *ms = mean duration of one launch; *points = grid points
+   covered by one launch. The pass is idempotent, so the state is unchanged. */
+int nls_pool_time_pass(nls_pool *pool, int32_t j, int32_t iters, float *ms, int64_t *points);
+/* Time `iters` whole steps of the pool without advancing trajectories is not
+   possible; steps are timed by the caller around nls_pool_step. */
+/* Launch counts of the most recent step: kernels launched per step. */
+int nls_pool_kernels_per_step(nls_pool *pool, int32_t *count);
+int nls_pool_destroy(nls_pool *pool);
+
+const char *nls_strerror(int code);
+/* Copy the calling thread's last error message (NUL-terminated). */
+int nls_last_error(char *buf, int32_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

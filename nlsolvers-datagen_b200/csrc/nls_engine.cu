@@ -1,0 +1,1149 @@
+// Host engine of the batched Lanczos exponential integrators and its C ABI
+// (include/nlsb200.h). A pool holds the device state of many trajectories
+// ("slots") of one (method, dim, k, precision); every step runs one fixed
+// launch sequence over a tile table of all unfinished slots, optionally
+// replayed as a CUDA graph. Snapshots stream to the callers' host buffers on a
+// copy stream while the next steps run.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/nlsb200.h"
+#include "nls_kernels.cuh"
+
+using namespace nlsb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(e_ == cudaErrorMemoryAllocation ? NLS_ERR_NO_MEMORY : NLS_ERR_CUDA, \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));               \
+  } while (0)
+
+constexpr int NF = 2;  // device snapshot frames per slot
+
+inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+// ---------------------------------------------------------- shared memory
+template <int DIM, typename E, int NSEQ> size_t smem_first() {
+  using G = Geo<DIM>;
+  using R = typename Traits<E>::R;
+  const size_t nv = NDot<E>::value * NSEQ;
+  size_t off = (size_t)NSEQ * 3 * G::PE * sizeof(E) + ((size_t)(G::D + 4) * G::PE + 2) * sizeof(R);
+  return align16(off) + 32 * nv * sizeof(double);
+}
+template <int DIM, typename E, int NSEQ> size_t smem_lanczos() {
+  using G = Geo<DIM>;
+  using R = typename Traits<E>::R;
+  const size_t nv = NDot<E>::value * NSEQ;
+  size_t off = (size_t)NSEQ * ((G::D + 4) + (G::D + 2) + 3) * G::PE * sizeof(E) +
+               (size_t)(G::D + 5) * G::PE * sizeof(R);
+  return align16(off) + 32 * nv * sizeof(double);
+}
+template <int DIM, typename E, int NSEQ> size_t smem_final() {
+  using G = Geo<DIM>;
+  using R = typename Traits<E>::R;
+  return (size_t)NSEQ * (G::D + 4) * G::PE * sizeof(E) + (size_t)(G::D + 4) * G::PE * sizeof(R);
+}
+template <int DIM, typename R> size_t smem_sv() {
+  using G = Geo<DIM>;
+  return (size_t)2 * (G::D + 4) * G::PE * sizeof(R);
+}
+
+template <typename K> cudaError_t set_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// ------------------------------------------------------------ kernel sets
+struct Launch {
+  // tile kernels take grid = tiles capacity; others compute their own grid
+  cudaError_t (*first)(const StepArgs &, int, cudaStream_t) = nullptr;
+  cudaError_t (*lanczos)(const StepArgs &, int, cudaStream_t) = nullptr;
+  cudaError_t (*final_)(const StepArgs &, int, cudaStream_t) = nullptr;
+};
+
+template <int DIM, typename E, int NSEQ, int SRC>
+cudaError_t launch_first(const StepArgs &a, int grid, cudaStream_t st) {
+  k_first<DIM, E, NSEQ, SRC><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_first<DIM, E, NSEQ>(), st>>>(a);
+  return cudaGetLastError();
+}
+template <int DIM, typename E, int NSEQ>
+cudaError_t launch_lanczos(const StepArgs &a, int grid, cudaStream_t st) {
+  k_lanczos<DIM, E, NSEQ><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_lanczos<DIM, E, NSEQ>(), st>>>(a);
+  return cudaGetLastError();
+}
+template <int DIM, typename E, int NSEQ, int FIN>
+cudaError_t launch_final(const StepArgs &a, int grid, cudaStream_t st) {
+  k_final<DIM, E, NSEQ, FIN><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_final<DIM, E, NSEQ>(), st>>>(a);
+  return cudaGetLastError();
+}
+template <int DIM, typename R> cudaError_t launch_sv(const StepArgs &a, int grid, cudaStream_t st) {
+  k_sv<DIM, R><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_sv<DIM, R>(), st>>>(a);
+  return cudaGetLastError();
+}
+template <typename E> cudaError_t launch_ftri(const StepArgs &a, int nslots_cap, cudaStream_t st) {
+  const int warps = nslots_cap * a.nseq;
+  k_ftri<E><<<(warps + 3) / 4, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template <typename E, int KIND>
+cudaError_t launch_ring(const StepArgs &a, int blocks_per_slot, int nslots_cap, cudaStream_t st) {
+  k_ring<E, KIND><<<dim3(blocks_per_slot, nslots_cap), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_advance(const StepArgs &a, int nslots_cap, cudaStream_t st) {
+  k_advance<<<(nslots_cap + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Kernel table of one (method family, dim, precision).
+struct KSet {
+  Launch kg, ss2, sewi_a, sewi_b;  // Gautschi / NLSE phases
+  cudaError_t (*sv)(const StepArgs &, int, cudaStream_t) = nullptr;
+  cudaError_t (*ftri)(const StepArgs &, int, cudaStream_t) = nullptr;
+  cudaError_t (*ring)(const StepArgs &, int, int, cudaStream_t) = nullptr;
+  cudaError_t (*set_attrs)() = nullptr;
+};
+
+template <int DIM, typename R> cudaError_t attrs_real() {
+  cudaError_t e;
+  if ((e = set_smem(k_first<DIM, R, 2, SRC_KG>, smem_first<DIM, R, 2>()))) return e;
+  if ((e = set_smem(k_lanczos<DIM, R, 2>, smem_lanczos<DIM, R, 2>()))) return e;
+  if ((e = set_smem(k_final<DIM, R, 2, FIN_KG>, smem_final<DIM, R, 2>()))) return e;
+  if ((e = set_smem(k_sv<DIM, R>, smem_sv<DIM, R>()))) return e;
+  return cudaSuccess;
+}
+template <int DIM, typename E> cudaError_t attrs_cplx() {
+  cudaError_t e;
+  if ((e = set_smem(k_first<DIM, E, 1, SRC_SS2>, smem_first<DIM, E, 1>()))) return e;
+  if ((e = set_smem(k_first<DIM, E, 2, SRC_SEWI_A>, smem_first<DIM, E, 2>()))) return e;
+  if ((e = set_smem(k_first<DIM, E, 1, SRC_SEWI_B>, smem_first<DIM, E, 1>()))) return e;
+  if ((e = set_smem(k_lanczos<DIM, E, 1>, smem_lanczos<DIM, E, 1>()))) return e;
+  if ((e = set_smem(k_lanczos<DIM, E, 2>, smem_lanczos<DIM, E, 2>()))) return e;
+  if ((e = set_smem(k_final<DIM, E, 1, FIN_SS2>, smem_final<DIM, E, 1>()))) return e;
+  if ((e = set_smem(k_final<DIM, E, 2, FIN_SEWI_A>, smem_final<DIM, E, 2>()))) return e;
+  if ((e = set_smem(k_final<DIM, E, 1, FIN_SEWI_B>, smem_final<DIM, E, 1>()))) return e;
+  return cudaSuccess;
+}
+
+template <int DIM, typename R> KSet make_real() {
+  KSet k;
+  k.kg.first = launch_first<DIM, R, 2, SRC_KG>;
+  k.kg.lanczos = launch_lanczos<DIM, R, 2>;
+  k.kg.final_ = launch_final<DIM, R, 2, FIN_KG>;
+  k.sv = launch_sv<DIM, R>;
+  k.ftri = launch_ftri<R>;
+  k.ring = launch_ring<R, 0>;
+  k.set_attrs = attrs_real<DIM, R>;
+  return k;
+}
+template <int DIM, typename E> KSet make_cplx() {
+  KSet k;
+  k.ss2.first = launch_first<DIM, E, 1, SRC_SS2>;
+  k.ss2.lanczos = launch_lanczos<DIM, E, 1>;
+  k.ss2.final_ = launch_final<DIM, E, 1, FIN_SS2>;
+  k.sewi_a.first = launch_first<DIM, E, 2, SRC_SEWI_A>;
+  k.sewi_a.lanczos = launch_lanczos<DIM, E, 2>;
+  k.sewi_a.final_ = launch_final<DIM, E, 2, FIN_SEWI_A>;
+  k.sewi_b.first = launch_first<DIM, E, 1, SRC_SEWI_B>;
+  k.sewi_b.lanczos = launch_lanczos<DIM, E, 1>;
+  k.sewi_b.final_ = launch_final<DIM, E, 1, FIN_SEWI_B>;
+  k.ftri = launch_ftri<E>;
+  k.ring = launch_ring<E, 1>;
+  k.set_attrs = attrs_cplx<DIM, E>;
+  return k;
+}
+
+KSet kset_for(int method, int dim, int prec) {
+  const bool cplx = method == NLS_NLSE_SS2 || method == NLS_NLSE_SEWI;
+  if (!cplx) {
+    if (dim == 2) return prec == NLS_FP64 ? make_real<2, double>() : make_real<2, float>();
+    return prec == NLS_FP64 ? make_real<3, double>() : make_real<3, float>();
+  }
+  if (dim == 2) return prec == NLS_FP64 ? make_cplx<2, Cx<double>>() : make_cplx<2, Cx<float>>();
+  return prec == NLS_FP64 ? make_cplx<3, Cx<double>>() : make_cplx<3, Cx<float>>();
+}
+
+bool is_cplx(int method) { return method == NLS_NLSE_SS2 || method == NLS_NLSE_SEWI; }
+bool is_sv(int method) { return method == NLS_KG_SV || method == NLS_SP4_SV; }
+bool is_krylov(int method) { return !is_sv(method); }
+
+// ------------------------------------------------------------ allocator
+struct Arena {
+  int64_t cap = 0;
+  std::map<int64_t, int64_t> free_;  // offset -> length
+  void init(int64_t c) {
+    cap = c;
+    free_.clear();
+    if (c > 0) free_[0] = c;
+  }
+  int64_t alloc(int64_t len) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= len) {
+        const int64_t off = it->first, rest = it->second - len;
+        free_.erase(it);
+        if (rest > 0) free_[off + len] = rest;
+        return off;
+      }
+    }
+    return -1;
+  }
+  void release(int64_t off, int64_t len) {
+    auto it = free_.emplace(off, len).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  int64_t free_total() const {
+    int64_t s = 0;
+    for (auto &kv : free_) s += kv.second;
+    return s;
+  }
+};
+
+struct SlotHost {
+  bool used = false;
+  nls_problem prob{};
+  int64_t off = 0, npad = 0, n = 0, snap_off = 0;
+  int step = 1;  // next step to run
+  int nt = 0, ns = 0, freq = 1;
+  double *traj = nullptr, *vel = nullptr;
+  bool reg_traj = false, reg_vel = false;
+  cudaEvent_t copy_done[NF] = {nullptr, nullptr};
+  bool copy_pending[NF] = {false, false};
+  bool needs_ss2 = false;  // SEWI: first step is a Strang step
+  int ring_cnt = 0;
+};
+
+struct TileSet {
+  TileDesc *d_tiles = nullptr;
+  int *d_ntiles = nullptr, *d_list = nullptr, *d_nlist = nullptr;
+  int cap = 0;       // allocated tiles
+  int live = 0;      // current tile count
+  int nlist = 0;
+  std::vector<TileDesc> tiles;
+  std::vector<int> list;
+};
+
+}  // namespace
+
+struct nls_pool {
+  int method = 0, dim = 2, k = 10, prec = NLS_FP32;
+  bool cplx = false;
+  int nseq_max = 2;
+  size_t esz = 4, rsz = 4;
+  int64_t cap = 0;
+  int max_slots = 0;
+  KSet ks;
+  Arena arena, snap_arena;
+  // device memory
+  void *u_hi = nullptr, *u_lo = nullptr, *u_alt = nullptr, *d = nullptr, *up_hi = nullptr,
+       *up_lo = nullptr, *ya = nullptr, *ib = nullptr, *m = nullptr, *c = nullptr, *V = nullptr;
+  double *snap = nullptr, *part = nullptr;
+  int part_tiles = 0;
+  SlotDesc *d_slots = nullptr;
+  SlotState *d_state = nullptr;
+  LzScal *d_scal = nullptr;
+  double *d_beta0 = nullptr;
+  FinalCoef *d_coef = nullptr;
+  TileSet main, first;  // main step / SEWI Strang first steps
+  std::vector<SlotHost> hs;
+  std::vector<SlotDesc> sd;
+  bool tables_dirty = true;
+  int seg2 = 32, seg3 = 16;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+  cudaEvent_t ev_step = nullptr;
+  bool use_graph = true;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_tiles = -1, graph_ring = -1;
+  int ring_blocks = 1;
+  int kernels_per_step = 0;
+  int device = 0;
+};
+
+struct nls_handle {
+  nls_pool *pool = nullptr;
+  int slot = -1;
+  nls_problem prob{};
+  int64_t n = 0;
+  double *traj = nullptr, *vel = nullptr;  // pinned
+};
+
+namespace {
+
+int64_t grid_points(const nls_problem &p) {
+  return (int64_t)p.nx * p.ny * (p.dim == 3 ? p.nz : 1);
+}
+
+int check_problem(const nls_problem *p) {
+  if (!p) return fail(NLS_ERR_INVALID_ARG, "null problem");
+  if (p->dim != 2 && p->dim != 3) return fail(NLS_ERR_INVALID_ARG, "dim must be 2 or 3");
+  if (p->nx < 3 || p->ny < 3 || (p->dim == 3 && p->nz < 3))
+    return fail(NLS_ERR_INVALID_ARG, "grid must be at least 3 points per axis");
+  if (p->method < 0 || p->method > NLS_NLSE_SEWI) return fail(NLS_ERR_INVALID_ARG, "unknown method");
+  if (p->nt <= 0 || p->ns <= 0 || p->nt / p->ns == 0)
+    return fail(NLS_ERR_INVALID_ARG, "need nt >= ns > 0 (snapshot period nt/ns is zero)");
+  if (is_krylov(p->method) && (p->k < 3 || p->k > KMAX))
+    return fail(NLS_ERR_INVALID_ARG, "Krylov dimension k must be in [3, 32]");
+  if (p->precision != NLS_FP32 && p->precision != NLS_FP64)
+    return fail(NLS_ERR_INVALID_ARG, "precision must be NLS_FP32 or NLS_FP64");
+  if (!(p->T > 0.0)) return fail(NLS_ERR_INVALID_ARG, "T must be positive");
+  const int64_t n = grid_points(*p);
+  if (n > (int64_t)1 << 31) return fail(NLS_ERR_INVALID_ARG, "grid too large (> 2^31 points)");
+  return NLS_OK;
+}
+
+void pool_free_device(nls_pool *P) {
+  void *bufs[] = {P->u_hi, P->u_lo, P->u_alt, P->d, P->up_hi, P->up_lo, P->ya, P->ib, P->m,
+                  P->c,    P->V,    P->snap,  P->part, P->d_slots, P->d_state, P->d_scal,
+                  P->d_beta0, P->d_coef, P->main.d_tiles, P->main.d_ntiles, P->main.d_list,
+                  P->main.d_nlist, P->first.d_tiles, P->first.d_ntiles, P->first.d_list,
+                  P->first.d_nlist};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+}
+
+int64_t slot_padded(const nls_problem &p, int32_t &pitch) {
+  pitch = (p.nx + 31) / 32 * 32;
+  const int64_t np = (int64_t)pitch * p.ny * (p.dim == 3 ? p.nz : 1);
+  return (np + 255) / 256 * 256;
+}
+
+// Tiles of one slot: 2-D: 128-wide column strips x seg rows; 3-D: 32x8 columns x seg planes.
+void slot_tiles(const nls_pool *P, int slot, const SlotDesc &s, std::vector<TileDesc> &out) {
+  const int tx = P->dim == 2 ? Geo<2>::TX : Geo<3>::TX;
+  const int ty = P->dim == 2 ? 1 : Geo<3>::TY;
+  const int np = P->dim == 2 ? s.ny : s.nz;
+  const int ny = P->dim == 2 ? 1 : s.ny;
+  const int seg = P->dim == 2 ? P->seg2 : P->seg3;
+  int local = 0;
+  for (int p0 = 0; p0 < np; p0 += seg)
+    for (int y0 = 0; y0 < ny; y0 += ty)
+      for (int x0 = 0; x0 < s.nx; x0 += tx) {
+        TileDesc t;
+        t.slot = slot;
+        t.x0 = x0;
+        t.y0 = y0;
+        t.p0 = p0;
+        t.p1 = std::min(np, p0 + seg);
+        t.local = local++;
+        out.push_back(t);
+      }
+}
+
+int ensure_tiles(nls_pool *P, TileSet &T, int need) {
+  if (need <= T.cap && T.d_tiles) return NLS_OK;
+  int cap = std::max(need, 64);
+  cap = (cap + 63) / 64 * 64;
+  if (T.d_tiles) cudaFree(T.d_tiles);
+  T.d_tiles = nullptr;
+  CK(cudaMalloc(&T.d_tiles, sizeof(TileDesc) * cap));
+  T.cap = cap;
+  return NLS_OK;
+}
+
+int ensure_partials(nls_pool *P, int tiles) {
+  if (tiles <= P->part_tiles && P->part) return NLS_OK;
+  const int nv = 2 * (P->cplx ? 9 : 6);
+  int cap = (std::max(tiles, 64) + 63) / 64 * 64;
+  if (P->part) cudaFree(P->part);
+  P->part = nullptr;
+  const int passes = std::max(P->k - 1, 1);
+  CK(cudaMalloc(&P->part, sizeof(double) * (size_t)passes * cap * nv));
+  P->part_tiles = cap;
+  P->gexec ? (void)0 : (void)0;
+  return NLS_OK;
+}
+
+// Rebuild the tile tables from the slots that still have steps to run.
+int rebuild_tables(nls_pool *P) {
+  P->main.tiles.clear();
+  P->main.list.clear();
+  P->first.tiles.clear();
+  P->first.list.clear();
+  int max_ring = 1;
+  for (int s = 0; s < P->max_slots; ++s) {
+    SlotHost &h = P->hs[s];
+    SlotDesc &d = P->sd[s];
+    d.active = h.used && h.step <= h.nt - 1;
+    if (!d.active) continue;
+    TileSet &T = (h.needs_ss2 && h.step == 1) ? P->first : P->main;
+    d.tile_begin = (int)T.tiles.size();
+    slot_tiles(P, s, d, T.tiles);
+    d.tile_count = (int)T.tiles.size() - d.tile_begin;
+    T.list.push_back(s);
+    max_ring = std::max(max_ring, h.ring_cnt);
+  }
+  int rb = 1;
+  while (rb * 256 * 4 < max_ring && rb < 256) rb *= 2;
+  P->ring_blocks = rb;
+  for (TileSet *T : {&P->main, &P->first}) {
+    T->live = (int)T->tiles.size();
+    T->nlist = (int)T->list.size();
+    int rc = ensure_tiles(P, *T, std::max(T->live, 1));
+    if (rc) return rc;
+    if (T->live) CK(cudaMemcpyAsync(T->d_tiles, T->tiles.data(), sizeof(TileDesc) * T->live, cudaMemcpyHostToDevice, P->stream));
+    CK(cudaMemcpyAsync(T->d_ntiles, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+    if (T->nlist) CK(cudaMemcpyAsync(T->d_list, T->list.data(), sizeof(int) * T->nlist, cudaMemcpyHostToDevice, P->stream));
+    CK(cudaMemcpyAsync(T->d_nlist, &T->nlist, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+  }
+  int rc = ensure_partials(P, std::max(P->main.cap, P->first.cap));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(P->d_slots, P->sd.data(), sizeof(SlotDesc) * P->max_slots, cudaMemcpyHostToDevice, P->stream));
+  // the pageable sources above are staged by the runtime before returning;
+  // synchronise only the stream ordering, not the host
+  P->tables_dirty = false;
+  return NLS_OK;
+}
+
+StepArgs base_args(const nls_pool *P, const TileSet &T) {
+  StepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.slots = P->d_slots;
+  a.state = P->d_state;
+  a.tiles = T.d_tiles;
+  a.ntiles = T.d_ntiles;
+  a.slot_list = T.d_list;
+  a.nslot_list = T.d_nlist;
+  a.f.u_hi = P->u_hi;
+  a.f.u_lo = P->u_lo;
+  a.f.u_alt = P->u_alt;
+  a.f.d = P->d;
+  a.f.up_hi = P->up_hi;
+  a.f.up_lo = P->up_lo;
+  a.f.ya = P->ya;
+  a.f.ib = P->ib;
+  a.f.m = P->m;
+  a.f.c = P->c;
+  a.f.snap = P->snap;
+  a.V = P->V;
+  a.vstride = P->cap;
+  a.k = P->k;
+  a.kv = P->k - 1;
+  a.part = P->part;
+  a.part_stride = (long long)P->part_tiles * 2 * (P->cplx ? 9 : 6);
+  a.scal = P->d_scal;
+  a.beta0 = P->d_beta0;
+  a.coef = P->d_coef;
+  return a;
+}
+
+// One Krylov application family (first pass, Lanczos passes, f(T), final).
+int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &nk) {
+  const int grid = T.cap;
+  CK(L.first(a, grid, P->stream));
+  ++nk;
+  for (int j = 1; j <= P->k - 2; ++j) {
+    a.j = j;
+    CK(L.lanczos(a, grid, P->stream));
+    ++nk;
+  }
+  CK(P->ks.ftri(a, P->max_slots, P->stream));
+  ++nk;
+  CK(L.final_(a, grid, P->stream));
+  ++nk;
+  return NLS_OK;
+}
+
+// The launch sequence of one step over tile set T. mode_first: SEWI Strang step.
+int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
+  int nk = 0;
+  StepArgs a = base_args(P, T);
+  const int m = P->method;
+  if (is_sv(m)) {
+    a.sv_pingpong = 1;
+    CK(P->ks.sv(a, T.cap, P->stream));
+    ++nk;
+  } else if (m == NLS_KG_GAUTSCHI || m == NLS_SP4_GAUTSCHI) {
+    // kg_single.cuh:103-111: cos(tau sqrt A) u and sinc^2(tau sqrt A) g(u), A = -L
+    a.nseq = 2;
+    a.op_sign = -1.0;
+    a.fkind[0] = FK_COS_SQRT;
+    a.fkind[1] = FK_SINC2_SQRT;
+    a.incr[0] = 1;
+    a.incr[1] = 0;
+    a.tsc[0][0] = 1.0;
+    a.tsc[1][0] = 1.0;
+    int rc = run_krylov(P, T, P->ks.kg, a, nk);
+    if (rc) return rc;
+  } else if (m == NLS_NLSE_SS2 || mode_first) {
+    // nlse_dev.hpp:190: exp(i dt L) with dti = (0, dt)
+    a.nseq = 1;
+    a.op_sign = 1.0;
+    a.fkind[0] = FK_EXP;
+    a.incr[0] = 1;
+    a.tsc[0][1] = 1.0;
+    int rc = run_krylov(P, T, P->ks.ss2, a, nk);
+    if (rc) return rc;
+  } else {
+    // nlse_dev.hpp:219-223: sinc(dt L) B(u) and exp(2 i dt L) u_prev, then exp(i dt L) y_a
+    a.nseq = 2;
+    a.op_sign = 1.0;
+    a.fkind[0] = FK_SINC;
+    a.fkind[1] = FK_EXP;
+    a.incr[0] = 0;
+    a.incr[1] = 1;
+    a.tsc[0][0] = 1.0;
+    a.tsc[1][1] = 2.0;
+    int rc = run_krylov(P, T, P->ks.sewi_a, a, nk);
+    if (rc) return rc;
+    StepArgs b = base_args(P, T);
+    b.nseq = 1;
+    b.op_sign = 1.0;
+    b.fkind[0] = FK_EXP;
+    b.incr[0] = 0;
+    b.tsc[0][1] = 1.0;
+    rc = run_krylov(P, T, P->ks.sewi_b, b, nk);
+    if (rc) return rc;
+  }
+  a.sv_pingpong = is_sv(m) ? 1 : 0;
+  CK(P->ks.ring(a, P->ring_blocks, P->max_slots, P->stream));
+  ++nk;
+  CK(launch_advance(a, P->max_slots, P->stream));
+  ++nk;
+  P->kernels_per_step = nk;
+  return NLS_OK;
+}
+
+int run_main_step(nls_pool *P) {
+  if (!P->use_graph) return enqueue_step(P, P->main, false);
+  if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks) {
+    if (P->gexec) {
+      cudaGraphExecDestroy(P->gexec);
+      P->gexec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(P, P->main, false);
+    cudaError_t e2 = cudaStreamEndCapture(P->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CK(e2);
+    cudaError_t e3 = cudaGraphInstantiate(&P->gexec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e3);
+    P->graph_tiles = P->main.cap;
+    P->graph_ring = P->ring_blocks;
+  }
+  CK(cudaGraphLaunch(P->gexec, P->stream));
+  return NLS_OK;
+}
+
+int wait_frame(nls_pool *P, SlotHost &h, int step) {
+  if (step % h.freq != 0 || step / h.freq >= h.ns) return NLS_OK;
+  const int f = (step / h.freq) % NF;
+  if (h.copy_pending[f]) CK(cudaStreamWaitEvent(P->stream, h.copy_done[f], 0));
+  return NLS_OK;
+}
+
+int issue_copies(nls_pool *P, SlotHost &h, const SlotDesc &d, int step) {
+  if (step % h.freq != 0 || step / h.freq >= h.ns) return NLS_OK;
+  const int si = step / h.freq, f = si % NF;
+  const double *frame = P->snap + d.snap_off + (int64_t)f * 2 * h.n;
+  if (P->cplx) {
+    CK(cudaMemcpyAsync(h.traj + (int64_t)si * 2 * h.n, frame, sizeof(double) * 2 * h.n,
+                       cudaMemcpyDeviceToHost, P->copy_stream));
+  } else {
+    CK(cudaMemcpyAsync(h.traj + (int64_t)si * h.n, frame, sizeof(double) * h.n,
+                       cudaMemcpyDeviceToHost, P->copy_stream));
+    if (h.vel)
+      CK(cudaMemcpyAsync(h.vel + (int64_t)si * h.n, frame + h.n, sizeof(double) * h.n,
+                         cudaMemcpyDeviceToHost, P->copy_stream));
+  }
+  CK(cudaEventRecord(h.copy_done[f], P->copy_stream));
+  h.copy_pending[f] = true;
+  return NLS_OK;
+}
+
+int pool_step_once(nls_pool *P) {
+  // slots whose step count is exhausted leave the tables
+  for (int s = 0; s < P->max_slots; ++s) {
+    const bool act = P->hs[s].used && P->hs[s].step <= P->hs[s].nt - 1;
+    if ((P->sd[s].active != 0) != act) P->tables_dirty = true;
+    if (P->hs[s].used && P->hs[s].needs_ss2 && P->hs[s].step == 2) {
+      P->hs[s].needs_ss2 = false;  // moves from the Strang table to the SEWI table
+      P->tables_dirty = true;
+    }
+  }
+  if (P->tables_dirty) {
+    int rc = rebuild_tables(P);
+    if (rc) return rc;
+  }
+  if (P->main.nlist == 0 && P->first.nlist == 0) return NLS_OK;
+  for (TileSet *T : {&P->first, &P->main})
+    for (int s : T->list) {
+      int rc = wait_frame(P, P->hs[s], P->hs[s].step);
+      if (rc) return rc;
+    }
+  if (P->first.nlist) {
+    int rc = enqueue_step(P, P->first, true);
+    if (rc) return rc;
+  }
+  if (P->main.nlist) {
+    int rc = run_main_step(P);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(P->ev_step, P->stream));
+  CK(cudaStreamWaitEvent(P->copy_stream, P->ev_step, 0));
+  for (TileSet *T : {&P->first, &P->main})
+    for (int s : T->list) {
+      SlotHost &h = P->hs[s];
+      int rc = issue_copies(P, h, P->sd[s], h.step);
+      if (rc) return rc;
+      h.step += 1;
+    }
+  return NLS_OK;
+}
+
+int upload_slot(nls_pool *P, int s, const double *u0, const double *v0, const double *m,
+                const double *c) {
+  SlotHost &h = P->hs[s];
+  const nls_problem &p = h.prob;
+  const SlotDesc &d = P->sd[s];
+  const int64_t np = h.npad;
+  const int nx = p.nx, ny = p.ny, nz = p.dim == 3 ? p.nz : 1;
+  const bool f32 = P->prec == NLS_FP32;
+  const int comps = P->cplx ? 2 : 1;
+  const double dt = p.T / p.nt;
+  std::vector<unsigned char> hi(np * P->esz, 0), lo(np * P->esz, 0), mr(np * P->rsz, 0),
+      cr(np * P->rsz, 0), dd;
+  if (!P->cplx) dd.assign(np * P->rsz, 0);
+  auto put = [&](std::vector<unsigned char> &buf, int64_t e, int comp, double v, bool real_buf) {
+    const int64_t idx = real_buf ? e : e * comps + comp;
+    if (f32)
+      reinterpret_cast<float *>(buf.data())[idx] = (float)v;
+    else
+      reinterpret_cast<double *>(buf.data())[idx] = v;
+  };
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const int64_t pt = ((int64_t)z * ny + y) * nx + x;
+        const int64_t e = ((int64_t)z * ny + y) * d.pitch + x;
+        for (int q = 0; q < comps; ++q) {
+          const double u = u0[pt * comps + q];
+          const double uh = f32 ? (double)(float)u : u;
+          put(hi, e, q, uh, false);
+          put(lo, e, q, u - uh, false);
+        }
+        put(mr, e, 0, m[pt], true);
+        if (p.has_c) put(cr, e, 0, c[pt], true);
+        if (!P->cplx) {
+          // u_past = u0 - dt v0 (kg_dev.hpp:55-58); d = u0 - u_past
+          const double vv = v0 ? v0[pt] : 0.0;
+          const double up = u0[pt] - dt * vv;
+          put(dd, e, 0, u0[pt] - up, true);
+        }
+      }
+  const int64_t eo = h.off;
+  CK(cudaMemcpyAsync((char *)P->u_hi + eo * P->esz, hi.data(), np * P->esz, cudaMemcpyHostToDevice, P->stream));
+  CK(cudaMemcpyAsync((char *)P->u_lo + eo * P->esz, lo.data(), np * P->esz, cudaMemcpyHostToDevice, P->stream));
+  CK(cudaMemcpyAsync((char *)P->m + eo * P->rsz, mr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
+  if (p.has_c) CK(cudaMemcpyAsync((char *)P->c + eo * P->rsz, cr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
+  if (!P->cplx) CK(cudaMemcpyAsync((char *)P->d + eo * P->rsz, dd.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
+  if (P->method == NLS_NLSE_SEWI) {
+    // u_prev <- u0 before the first (Strang) step (nlse_dev.hpp:206-209)
+    CK(cudaMemcpyAsync((char *)P->up_hi + eo * P->esz, (char *)P->u_hi + eo * P->esz, np * P->esz, cudaMemcpyDeviceToDevice, P->stream));
+    CK(cudaMemcpyAsync((char *)P->up_lo + eo * P->esz, (char *)P->u_lo + eo * P->esz, np * P->esz, cudaMemcpyDeviceToDevice, P->stream));
+  }
+  SlotState st{1, 1, 0, 0};
+  CK(cudaMemcpyAsync(P->d_state + s, &st, sizeof(SlotState), cudaMemcpyHostToDevice, P->stream));
+  // the host vectors are staged by the runtime before each call returns
+  return NLS_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+const char *nls_strerror(int code) {
+  switch (code) {
+  case NLS_OK: return "ok";
+  case NLS_ERR_INVALID_ARG: return "invalid argument";
+  case NLS_ERR_SHAPE: return "shape mismatch";
+  case NLS_ERR_NO_MEMORY: return "out of memory";
+  case NLS_ERR_CUDA: return "CUDA error";
+  case NLS_ERR_NO_DEVICE: return "no CUDA device";
+  case NLS_ERR_CAPACITY: return "pool capacity exhausted";
+  case NLS_ERR_STATE: return "invalid state";
+  case NLS_ERR_NUMERIC: return "numerical failure";
+  case NLS_ERR_IO: return "I/O error";
+  }
+  return "unknown error";
+}
+
+int nls_last_error(char *buf, int32_t len) {
+  if (!buf || len <= 0) return NLS_ERR_INVALID_ARG;
+  std::snprintf(buf, (size_t)len, "%s", g_err.c_str());
+  return NLS_OK;
+}
+
+int nls_problem_defaults(nls_problem *p, int32_t method, int32_t dim) {
+  if (!p) return fail(NLS_ERR_INVALID_ARG, "null problem");
+  std::memset(p, 0, sizeof(*p));
+  p->dim = dim;
+  p->method = method;
+  p->precision = NLS_FP32;
+  p->has_c = 1;
+  switch (method) {
+  case NLS_KG_GAUTSCHI:
+  case NLS_KG_SV:
+    p->p3 = -1.0;  // -m u^3 (kg_single.cuh:106-109, 152-155)
+    p->k = 10;     // kg_driver_dev_2d.cpp:138
+    break;
+  case NLS_SP4_SV:
+  case NLS_SP4_GAUTSCHI:
+    p->p1 = -1.0;  // -m (u - u^3 + s xi) (stochastic_phi4.cuh:52)
+    p->p3 = 1.0;
+    p->k = 10;
+    break;  // rm = -s is set by the caller from dx and dt
+  case NLS_NLSE_SS2:
+    p->p3 = 1.0;  // rho = m |u|^2 (nlse_dev.hpp:27)
+    p->k = dim == 2 ? 20 : 25;  // nlse_cubic_driver_{2d:104, 3d:112}
+    break;
+  case NLS_NLSE_SEWI:
+    p->p3 = 1.0;
+    p->k = dim == 2 ? 10 : 15;  // nlse_cubic_sewi_driver_{2d:104, 3d:112}
+    break;
+  default:
+    return fail(NLS_ERR_INVALID_ARG, "unknown method");
+  }
+  return NLS_OK;
+}
+
+int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
+                    int64_t capacity_points, int32_t max_slots, nls_pool **out) {
+  if (!out) return fail(NLS_ERR_INVALID_ARG, "null out");
+  *out = nullptr;
+  if (method < 0 || method > NLS_NLSE_SEWI) return fail(NLS_ERR_INVALID_ARG, "unknown method");
+  if (dim != 2 && dim != 3) return fail(NLS_ERR_INVALID_ARG, "dim must be 2 or 3");
+  if (is_krylov(method) && (k < 3 || k > KMAX)) return fail(NLS_ERR_INVALID_ARG, "k must be in [3, 32]");
+  if (precision != NLS_FP32 && precision != NLS_FP64) return fail(NLS_ERR_INVALID_ARG, "bad precision");
+  if (capacity_points <= 0 || max_slots <= 0) return fail(NLS_ERR_INVALID_ARG, "empty capacity");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(NLS_ERR_NO_DEVICE, "no CUDA device available");
+  nls_pool *P = new (std::nothrow) nls_pool();
+  if (!P) return fail(NLS_ERR_NO_MEMORY, "host allocation failed");
+  cudaGetDevice(&P->device);
+  P->method = method;
+  P->dim = dim;
+  P->k = is_krylov(method) ? k : 3;
+  P->prec = precision;
+  P->cplx = is_cplx(method);
+  P->nseq_max = method == NLS_NLSE_SS2 ? 1 : 2;
+  P->rsz = precision == NLS_FP64 ? 8 : 4;
+  P->esz = P->rsz * (P->cplx ? 2 : 1);
+  P->cap = (capacity_points + 255) / 256 * 256;
+  P->max_slots = max_slots;
+  P->ks = kset_for(method, dim, precision);
+  P->arena.init(P->cap);
+  P->snap_arena.init(P->cap * 2 * NF);
+  P->hs.assign(max_slots, SlotHost());
+  P->sd.assign(max_slots, SlotDesc());
+  int rc = NLS_OK;
+  auto al = [&](void **p, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess)
+      return fail(NLS_ERR_NO_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return NLS_OK;
+  };
+  const size_t ce = (size_t)P->cap;
+  if (!rc) rc = al(&P->u_hi, ce * P->esz);
+  if (!rc) rc = al(&P->u_lo, ce * P->esz);
+  if (!rc) rc = al(&P->m, ce * P->rsz);
+  if (!rc) rc = al(&P->c, ce * P->rsz);
+  if (!rc && !P->cplx) rc = al(&P->d, ce * P->rsz);
+  if (!rc && is_sv(method)) rc = al(&P->u_alt, ce * P->esz);
+  if (!rc && method == NLS_NLSE_SEWI) {
+    rc = al(&P->up_hi, ce * P->esz);
+    if (!rc) rc = al(&P->up_lo, ce * P->esz);
+    if (!rc) rc = al(&P->ya, ce * P->esz);
+    if (!rc) rc = al(&P->ib, ce * P->esz);
+  }
+  if (!rc && is_krylov(method)) rc = al(&P->V, ce * P->esz * (size_t)P->nseq_max * (P->k - 1));
+  if (!rc) rc = al((void **)&P->snap, sizeof(double) * ce * 2 * NF);
+  if (!rc) rc = al((void **)&P->d_slots, sizeof(SlotDesc) * max_slots);
+  if (!rc) rc = al((void **)&P->d_state, sizeof(SlotState) * max_slots);
+  if (!rc) rc = al((void **)&P->d_scal, sizeof(LzScal) * max_slots * 2 * KMAX);
+  if (!rc) rc = al((void **)&P->d_beta0, sizeof(double) * max_slots * 2);
+  if (!rc) rc = al((void **)&P->d_coef, sizeof(FinalCoef) * max_slots * 2);
+  for (TileSet *T : {&P->main, &P->first}) {
+    if (!rc) rc = al((void **)&T->d_ntiles, sizeof(int));
+    if (!rc) rc = al((void **)&T->d_nlist, sizeof(int));
+    if (!rc) rc = al((void **)&T->d_list, sizeof(int) * max_slots);
+  }
+  if (!rc && P->ks.set_attrs) {
+    cudaError_t e = P->ks.set_attrs();
+    if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  }
+  if (!rc && cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "stream");
+  if (!rc && cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "stream");
+  if (!rc && cudaEventCreateWithFlags(&P->ev_step, cudaEventDisableTiming) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "event");
+  if (!rc) {
+    cudaError_t e = cudaMemsetAsync(P->d_state, 0, sizeof(SlotState) * max_slots, P->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->snap, 0, sizeof(double) * ce * 2 * NF, P->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->d_coef, 0, sizeof(FinalCoef) * max_slots * 2, P->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
+    if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (rc) {
+    pool_free_device(P);
+    if (P->stream) cudaStreamDestroy(P->stream);
+    if (P->copy_stream) cudaStreamDestroy(P->copy_stream);
+    if (P->ev_step) cudaEventDestroy(P->ev_step);
+    delete P;
+    return rc;
+  }
+  *out = P;
+  return NLS_OK;
+}
+
+int nls_pool_admit(nls_pool *P, const nls_problem *p, const double *u0, const double *v0,
+                   const double *m, const double *c, double *traj_dst, double *vel_dst,
+                   int32_t *slot_out) {
+  if (!P || !slot_out) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  int rc = check_problem(p);
+  if (rc) return rc;
+  if (p->method != P->method || p->dim != P->dim || p->precision != P->prec ||
+      (is_krylov(p->method) && p->k != P->k))
+    return fail(NLS_ERR_INVALID_ARG, "problem does not match the pool (method, dim, k, precision)");
+  if (!u0 || !m || !traj_dst || (p->has_c && !c))
+    return fail(NLS_ERR_INVALID_ARG, "missing input array");
+  int s = -1;
+  for (int q = 0; q < P->max_slots; ++q)
+    if (!P->hs[q].used) {
+      s = q;
+      break;
+    }
+  if (s < 0) return fail(NLS_ERR_CAPACITY, "no free slot");
+  int32_t pitch = 0;
+  const int64_t npad = slot_padded(*p, pitch);
+  const int64_t n = grid_points(*p);
+  const int64_t off = P->arena.alloc(npad);
+  if (off < 0) return fail(NLS_ERR_CAPACITY, "not enough free device points in the pool");
+  const int64_t soff = P->snap_arena.alloc(2 * NF * n);
+  if (soff < 0) {
+    P->arena.release(off, npad);
+    return fail(NLS_ERR_CAPACITY, "not enough snapshot memory in the pool");
+  }
+  SlotHost &h = P->hs[s];
+  h = SlotHost();
+  h.used = true;
+  h.prob = *p;
+  h.off = off;
+  h.npad = npad;
+  h.n = n;
+  h.snap_off = soff;
+  h.step = 1;
+  h.nt = p->nt;
+  h.ns = p->ns;
+  h.freq = p->nt / p->ns;
+  h.traj = traj_dst;
+  h.vel = P->cplx ? nullptr : vel_dst;
+  h.needs_ss2 = p->method == NLS_NLSE_SEWI;
+  h.ring_cnt = (int)std::min<long long>(ring_count(p->dim, p->nx, p->ny, p->nz), 1LL << 30);
+  const size_t tb = sizeof(double) * (size_t)n * p->ns * (P->cplx ? 2 : 1);
+  h.reg_traj = cudaHostRegister(traj_dst, tb, cudaHostRegisterDefault) == cudaSuccess;
+  if (h.vel) h.reg_vel = cudaHostRegister(h.vel, sizeof(double) * (size_t)n * p->ns, cudaHostRegisterDefault) == cudaSuccess;
+  cudaGetLastError();  // a failed registration only makes the copies synchronous
+  for (int f = 0; f < NF; ++f)
+    if (cudaEventCreateWithFlags(&h.copy_done[f], cudaEventDisableTiming) != cudaSuccess)
+      return fail(NLS_ERR_CUDA, "event");
+  SlotDesc &d = P->sd[s];
+  std::memset(&d, 0, sizeof(d));
+  const double dx = 2 * p->Lx / (p->nx - 1), dy = 2 * p->Ly / (p->ny - 1);
+  d.dim = p->dim;
+  d.nx = p->nx;
+  d.ny = p->ny;
+  d.nz = p->dim == 3 ? p->nz : 1;
+  d.pitch = pitch;
+  d.has_c = p->has_c ? 1 : 0;
+  d.off = off;
+  d.inv_h2 = p->dim == 2 ? 1.0 / (dx * dy) : 1.0 / (dx * dx);
+  d.dt = p->T / p->nt;
+  d.p1 = p->p1;
+  d.q1 = p->q1;
+  d.p3 = p->p3;
+  d.q3 = p->q3;
+  d.rm = p->rm;
+  d.r0 = p->r0;
+  d.seed = p->seed;
+  d.nt = p->nt;
+  d.ns = p->ns;
+  d.freq = h.freq;
+  d.snap_frames = NF;
+  d.snap_off = soff;
+  d.n = n;
+  d.active = 0;
+  d.variant = p->sewi_variant;
+  // snapshot 0 is the initial state (kg_dev.hpp:263, nlse_cubic_driver_2d.cpp:106)
+  if (P->cplx) {
+    std::memcpy(traj_dst, u0, sizeof(double) * 2 * n);
+  } else {
+    std::memcpy(traj_dst, u0, sizeof(double) * n);
+    if (h.vel) {
+      if (v0)
+        std::memcpy(h.vel, v0, sizeof(double) * n);
+      else
+        std::memset(h.vel, 0, sizeof(double) * n);
+    }
+  }
+  rc = upload_slot(P, s, u0, v0, m, c);
+  if (rc) return rc;
+  P->tables_dirty = true;
+  *slot_out = s;
+  return NLS_OK;
+}
+
+int nls_pool_step(nls_pool *P, int32_t nsteps) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = pool_step_once(P);
+    if (rc) return rc;
+  }
+  return NLS_OK;
+}
+
+int nls_pool_poll(nls_pool *P, int32_t s, int32_t *steps_done, int32_t *finished) {
+  if (!P || s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
+  SlotHost &h = P->hs[s];
+  if (steps_done) *steps_done = h.step - 1;
+  if (finished) {
+    bool fin = h.step > h.nt - 1;
+    for (int f = 0; f < NF && fin; ++f) {
+      if (h.copy_pending[f]) {
+        cudaError_t e = cudaEventQuery(h.copy_done[f]);
+        if (e == cudaErrorNotReady) {
+          fin = false;
+        } else if (e != cudaSuccess) {
+          return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
+        }
+      }
+    }
+    *finished = fin ? 1 : 0;
+  }
+  return NLS_OK;
+}
+
+int nls_pool_release(nls_pool *P, int32_t s) {
+  if (!P || s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
+  SlotHost &h = P->hs[s];
+  for (int f = 0; f < NF; ++f) {
+    if (h.copy_pending[f]) CK(cudaEventSynchronize(h.copy_done[f]));
+    if (h.copy_done[f]) cudaEventDestroy(h.copy_done[f]);
+  }
+  // the slot's memory is reused by later admissions only after queued steps
+  CK(cudaStreamSynchronize(P->stream));
+  if (h.reg_traj) cudaHostUnregister(h.traj);
+  if (h.reg_vel) cudaHostUnregister(h.vel);
+  P->arena.release(h.off, h.npad);
+  P->snap_arena.release(h.snap_off, 2 * NF * h.n);
+  h = SlotHost();
+  P->sd[s].active = 0;
+  P->tables_dirty = true;
+  return NLS_OK;
+}
+
+int nls_pool_sync(nls_pool *P) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  CK(cudaStreamSynchronize(P->stream));
+  CK(cudaStreamSynchronize(P->copy_stream));
+  // device-side status (eigensolver convergence)
+  std::vector<SlotState> st(P->max_slots);
+  CK(cudaMemcpy(st.data(), P->d_state, sizeof(SlotState) * P->max_slots, cudaMemcpyDeviceToHost));
+  for (int s = 0; s < P->max_slots; ++s)
+    if (P->hs[s].used && st[s].status != 0)
+      return fail(NLS_ERR_NUMERIC, "tridiagonal eigensolver did not converge for slot " + std::to_string(s));
+  return NLS_OK;
+}
+
+int nls_pool_usage(nls_pool *P, int32_t *occupied, int64_t *free_points) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  int occ = 0;
+  for (auto &h : P->hs) occ += h.used ? 1 : 0;
+  if (occupied) *occupied = occ;
+  if (free_points) *free_points = P->arena.free_total();
+  return NLS_OK;
+}
+
+int nls_pool_set_graphs(nls_pool *P, int32_t enable) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  P->use_graph = enable != 0;
+  return NLS_OK;
+}
+
+int nls_pool_set_segment(nls_pool *P, int32_t rows) {
+  if (!P || rows < 1) return fail(NLS_ERR_INVALID_ARG, "bad segment");
+  if (P->dim == 2)
+    P->seg2 = rows;
+  else
+    P->seg3 = rows;
+  P->tables_dirty = true;
+  return NLS_OK;
+}
+
+int nls_pool_kernels_per_step(nls_pool *P, int32_t *count) {
+  if (!P || !count) return fail(NLS_ERR_INVALID_ARG, "null");
+  *count = P->kernels_per_step;
+  return NLS_OK;
+}
+
+int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t *points) {
+  if (!P || !ms || iters <= 0) return fail(NLS_ERR_INVALID_ARG, "null");
+  if (!is_krylov(P->method) || j < 1 || j > P->k - 2) return fail(NLS_ERR_INVALID_ARG, "bad pass index");
+  if (P->tables_dirty) {
+    int rc = rebuild_tables(P);
+    if (rc) return rc;
+  }
+  if (P->main.nlist == 0) return fail(NLS_ERR_STATE, "no active slot");
+  StepArgs a = base_args(P, P->main);
+  a.j = j;
+  a.op_sign = P->cplx ? 1.0 : -1.0;
+  const Launch &L = P->cplx ? (P->method == NLS_NLSE_SS2 ? P->ks.ss2 : P->ks.sewi_a) : P->ks.kg;
+  a.nseq = P->method == NLS_NLSE_SS2 ? 1 : 2;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(L.lanczos(a, P->main.cap, P->stream));  // warm
+  CK(cudaEventRecord(e0, P->stream));
+  for (int i = 0; i < iters; ++i) CK(L.lanczos(a, P->main.cap, P->stream));
+  CK(cudaEventRecord(e1, P->stream));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / iters;
+  if (points) {
+    int64_t pts = 0;
+    for (int s : P->main.list) pts += P->hs[s].n;
+    *points = pts;
+  }
+  return NLS_OK;
+}
+
+int nls_pool_destroy(nls_pool *P) {
+  if (!P) return NLS_OK;
+  cudaStreamSynchronize(P->stream);
+  cudaStreamSynchronize(P->copy_stream);
+  for (auto &h : P->hs) {
+    if (!h.used) continue;
+    for (int f = 0; f < NF; ++f)
+      if (h.copy_done[f]) cudaEventDestroy(h.copy_done[f]);
+    if (h.reg_traj) cudaHostUnregister(h.traj);
+    if (h.reg_vel) cudaHostUnregister(h.vel);
+  }
+  if (P->gexec) cudaGraphExecDestroy(P->gexec);
+  pool_free_device(P);
+  cudaStreamDestroy(P->stream);
+  cudaStreamDestroy(P->copy_stream);
+  cudaEventDestroy(P->ev_step);
+  delete P;
+  return NLS_OK;
+}
+
+// ------------------------------------------------------ single trajectory
+int nls_create(const nls_problem *p, const double *u0, const double *v0, const double *m,
+               const double *c, nls_handle **out) {
+  if (!out) return fail(NLS_ERR_INVALID_ARG, "null out");
+  *out = nullptr;
+  int rc = check_problem(p);
+  if (rc) return rc;
+  nls_handle *H = new (std::nothrow) nls_handle();
+  if (!H) return fail(NLS_ERR_NO_MEMORY, "host allocation failed");
+  H->prob = *p;
+  H->n = grid_points(*p);
+  const size_t tb = sizeof(double) * (size_t)H->n * p->ns * (is_cplx(p->method) ? 2 : 1);
+  int32_t pitch;
+  const int64_t npad = slot_padded(*p, pitch);
+  rc = nls_pool_create(p->method, p->dim, p->k, p->precision, npad, 1, &H->pool);
+  if (rc) {
+    delete H;
+    return rc;
+  }
+  if (cudaMallocHost(&H->traj, tb) != cudaSuccess ||
+      (!is_cplx(p->method) && cudaMallocHost(&H->vel, sizeof(double) * H->n * p->ns) != cudaSuccess)) {
+    nls_destroy(H);
+    return fail(NLS_ERR_NO_MEMORY, "pinned host allocation failed");
+  }
+  rc = nls_pool_admit(H->pool, p, u0, v0, m, c, H->traj, H->vel, &H->slot);
+  if (rc) {
+    std::string keep = g_err;
+    nls_destroy(H);
+    g_err = keep;
+    return rc;
+  }
+  *out = H;
+  return NLS_OK;
+}
+
+int nls_step(nls_handle *H, int32_t nsteps) {
+  if (!H) return fail(NLS_ERR_INVALID_ARG, "null handle");
+  return nls_pool_step(H->pool, nsteps);
+}
+
+int nls_run(nls_handle *H) {
+  if (!H) return fail(NLS_ERR_INVALID_ARG, "null handle");
+  const int left = H->prob.nt - H->pool->hs[H->slot].step;
+  return nls_pool_step(H->pool, std::max(left, 0));
+}
+
+int nls_steps_done(nls_handle *H, int32_t *steps) {
+  if (!H || !steps) return fail(NLS_ERR_INVALID_ARG, "null");
+  *steps = H->pool->hs[H->slot].step - 1;
+  return NLS_OK;
+}
+
+int nls_snapshot(nls_handle *H, double *traj, double *vel) {
+  if (!H || !traj) return fail(NLS_ERR_INVALID_ARG, "null");
+  int rc = nls_pool_sync(H->pool);
+  if (rc) return rc;
+  const size_t tb = sizeof(double) * (size_t)H->n * H->prob.ns * (is_cplx(H->prob.method) ? 2 : 1);
+  std::memcpy(traj, H->traj, tb);
+  if (vel && H->vel) std::memcpy(vel, H->vel, sizeof(double) * (size_t)H->n * H->prob.ns);
+  return NLS_OK;
+}
+
+int nls_destroy(nls_handle *H) {
+  if (!H) return NLS_OK;
+  if (H->pool) {
+    if (H->slot >= 0) nls_pool_release(H->pool, H->slot);
+    nls_pool_destroy(H->pool);
+  }
+  if (H->traj) cudaFreeHost(H->traj);
+  if (H->vel) cudaFreeHost(H->vel);
+  delete H;
+  return NLS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,256 @@
+"""Python mirror of the reference's solver interface, over the C ABI.
+
+``Solver`` replaces one reference solver object plus its driver loop
+(``KGESolverDevice`` kg_dev.hpp:32-131, ``SP4SolverDevice``
+stochastic_phi4_dev.hpp:29-33, ``NLSESolverDevice`` nlse_dev.hpp:78-335, loop
+kg_driver_dev_2d.cpp:144-153). ``Pool`` is the batched / continuous-batching
+engine many trajectories share.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import (FP32, FP64, KG_GAUTSCHI, KG_SV, NLSE_SEWI, NLSE_SS2, SP4_GAUTSCHI, SP4_SV,
+                   NlsError, check, lib)
+
+COMPLEX_METHODS = (NLSE_SS2, NLSE_SEWI)
+KRYLOV_METHODS = (KG_GAUTSCHI, SP4_GAUTSCHI, NLSE_SS2, NLSE_SEWI)
+
+
+@dataclass
+class Spec:
+    """Problem description; grid sizes include the ghost ring (driver argv)."""
+    method: int
+    dim: int
+    nx: int
+    ny: int
+    nz: int = 1
+    Lx: float = 10.0
+    Ly: float = 10.0
+    Lz: float = 10.0
+    T: float = 1.0
+    nt: int = 100
+    ns: int = 10
+    k: int | None = None
+    precision: int = FP32
+    sewi_variant: int = 0
+    p1: float | None = None
+    q1: float = 0.0
+    p3: float | None = None
+    q3: float = 0.0
+    rm: float | None = None
+    r0: float = 0.0
+    seed: int = 0
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx) if self.dim == 3 else (self.ny, self.nx)
+
+    @property
+    def n(self):
+        return int(np.prod(self.shape))
+
+    @property
+    def dt(self):
+        return self.T / self.nt
+
+    @property
+    def complex(self):
+        return self.method in COMPLEX_METHODS
+
+    def struct(self, has_c: bool) -> _lib.Problem:
+        p = _lib.Problem()
+        check(lib().nls_problem_defaults(ctypes.byref(p), self.method, self.dim))
+        p.nx, p.ny, p.nz = self.nx, self.ny, (self.nz if self.dim == 3 else 1)
+        p.Lx, p.Ly, p.Lz = self.Lx, self.Ly, self.Lz
+        p.T, p.nt, p.ns = self.T, self.nt, self.ns
+        if self.k is not None:
+            p.k = self.k
+        p.precision = self.precision
+        p.sewi_variant = self.sewi_variant
+        p.has_c = 1 if has_c else 0
+        if self.p1 is not None:
+            p.p1 = self.p1
+        if self.p3 is not None:
+            p.p3 = self.p3
+        p.q1, p.q3, p.r0 = self.q1, self.q3, self.r0
+        if self.rm is not None:
+            p.rm = self.rm
+        elif self.method in (SP4_SV, SP4_GAUTSCHI):
+            p.rm = reference_phi4_rm(self)
+        p.seed = self.seed
+        return p
+
+    def oracle_params(self):
+        """Nonlinearity coefficients as the library resolves them."""
+        s = self.struct(False)
+        return dict(k=s.k, p1=s.p1, q1=s.q1, p3=s.p3, q3=s.q3, rm=s.rm, r0=s.r0)
+
+
+def reference_phi4_rm(spec: Spec) -> float:
+    """-alpha sqrt(kBT dx)/dt with alpha = 0.01, kBT = 2, dx = 2L/(nx-1)
+    (stochastic_phi4_dev.hpp:47-51): the noise enters as -m s xi."""
+    dx = 2 * spec.Lx / (spec.nx - 1)
+    return -(0.01 * math.sqrt(2.0 * dx) / spec.dt)
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _prep(spec: Spec, u0, v0, m, c):
+    shape = spec.shape
+    u0 = np.ascontiguousarray(np.reshape(u0, shape),
+                              dtype=np.complex128 if spec.complex else np.float64)
+    v0 = None if (v0 is None or spec.complex) else np.ascontiguousarray(np.reshape(v0, shape), dtype=np.float64)
+    m = np.ascontiguousarray(np.reshape(m, shape), dtype=np.float64)
+    has_c = c is not None and not np.all(np.asarray(c) == 1.0)
+    c = np.ascontiguousarray(np.reshape(c, shape), dtype=np.float64) if has_c else None
+    return u0, v0, m, c, has_c
+
+
+class Solver:
+    """One trajectory on the GPU: snapshot 0 is the input; ``run()`` executes
+    the driver loop i = 1..nt-1; ``snapshots()`` returns (traj, vel)."""
+
+    def __init__(self, spec: Spec, u0, v0, m, c=None):
+        self.spec = spec
+        u0, v0, m, c, has_c = _prep(spec, u0, v0, m, c)
+        self._keep = (u0, v0, m, c)
+        self._h = ctypes.c_void_p()
+        check(lib().nls_create(ctypes.byref(spec.struct(has_c)), _dptr(u0.view(np.float64)),
+                               _dptr(v0), _dptr(m), _dptr(c), ctypes.byref(self._h)))
+
+    def step(self, nsteps: int = 1):
+        check(lib().nls_step(self._h, nsteps))
+
+    def run(self):
+        check(lib().nls_run(self._h))
+
+    def steps_done(self) -> int:
+        v = ctypes.c_int32()
+        check(lib().nls_steps_done(self._h, ctypes.byref(v)))
+        return v.value
+
+    def snapshots(self):
+        s = self.spec
+        traj = np.zeros((s.ns,) + s.shape, dtype=np.complex128 if s.complex else np.float64)
+        vel = None if s.complex else np.zeros((s.ns,) + s.shape)
+        check(lib().nls_snapshot(self._h, _dptr(traj.view(np.float64)), _dptr(vel)))
+        return traj, vel
+
+    def close(self):
+        if self._h:
+            lib().nls_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+@dataclass
+class SlotInfo:
+    slot: int
+    spec: Spec
+    traj: np.ndarray
+    vel: np.ndarray | None
+    inputs: tuple = field(default_factory=tuple)
+
+
+class Pool:
+    """Batched engine: trajectories of one (method, dim, k, precision) with any
+    grid sizes step together; admit/release between steps."""
+
+    def __init__(self, method: int, dim: int, k: int | None, precision: int,
+                 capacity_points: int, max_slots: int, graphs: bool = True,
+                 segment: int | None = None):
+        if k is None:
+            p = _lib.Problem()
+            check(lib().nls_problem_defaults(ctypes.byref(p), method, dim))
+            k = p.k
+        self.method, self.dim, self.k, self.precision = method, dim, k, precision
+        self._p = ctypes.c_void_p()
+        check(lib().nls_pool_create(method, dim, k, precision, int(capacity_points),
+                                    int(max_slots), ctypes.byref(self._p)))
+        self.slots: dict[int, SlotInfo] = {}
+        if not graphs:
+            check(lib().nls_pool_set_graphs(self._p, 0))
+        if segment:
+            check(lib().nls_pool_set_segment(self._p, int(segment)))
+
+    def admit(self, spec: Spec, u0, v0, m, c=None, traj=None, vel=None):
+        """Returns the slot id, or None when the pool is full right now."""
+        u0, v0, m, c, has_c = _prep(spec, u0, v0, m, c)
+        if traj is None:
+            traj = np.zeros((spec.ns,) + spec.shape,
+                            dtype=np.complex128 if spec.complex else np.float64)
+        if vel is None and not spec.complex:
+            vel = np.zeros((spec.ns,) + spec.shape)
+        slot = ctypes.c_int32(-1)
+        rc = lib().nls_pool_admit(self._p, ctypes.byref(spec.struct(has_c)),
+                                  _dptr(u0.view(np.float64)), _dptr(v0), _dptr(m), _dptr(c),
+                                  _dptr(traj.view(np.float64)), _dptr(vel), ctypes.byref(slot))
+        if rc == _lib.NLS_ERR_CAPACITY:
+            return None
+        check(rc)
+        self.slots[slot.value] = SlotInfo(slot.value, spec, traj, vel, (u0, v0, m, c))
+        return slot.value
+
+    def step(self, nsteps: int = 1):
+        check(lib().nls_pool_step(self._p, int(nsteps)))
+
+    def poll(self, slot: int):
+        done, fin = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().nls_pool_poll(self._p, slot, ctypes.byref(done), ctypes.byref(fin)))
+        return done.value, bool(fin.value)
+
+    def release(self, slot: int) -> SlotInfo:
+        check(lib().nls_pool_release(self._p, slot))
+        return self.slots.pop(slot)
+
+    def sync(self):
+        check(lib().nls_pool_sync(self._p))
+
+    def usage(self):
+        occ, free = ctypes.c_int32(), ctypes.c_int64()
+        check(lib().nls_pool_usage(self._p, ctypes.byref(occ), ctypes.byref(free)))
+        return occ.value, free.value
+
+    def time_pass(self, j: int, iters: int):
+        ms, pts = ctypes.c_float(), ctypes.c_int64()
+        check(lib().nls_pool_time_pass(self._p, j, iters, ctypes.byref(ms), ctypes.byref(pts)))
+        return ms.value, pts.value
+
+    def kernels_per_step(self) -> int:
+        v = ctypes.c_int32()
+        check(lib().nls_pool_kernels_per_step(self._p, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if self._p:
+            lib().nls_pool_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["Spec", "Solver", "Pool", "NlsError", "KG_GAUTSCHI", "KG_SV", "SP4_SV",
+           "SP4_GAUTSCHI", "NLSE_SS2", "NLSE_SEWI", "FP32", "FP64", "reference_phi4_rm"]

@@ -1,0 +1,103 @@
+/*
+ * FP64 CPU oracle for the Lanczos exponential integrators of
+ * konradha/nlsolvers-datagen (device/include + device/drivers).
+ *
+ * TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py may load this library, and
+ * only as the checker or the timed CPU baseline. The product never links it.
+ *
+ * PARITY UNPINNED: the reference ships no tests, golden vectors or fixtures,
+ * has no CPU implementation, and cannot be built here (Eigen3 and the libnpy
+ * submodule are absent; its only code path is CUDA). This file is a line-level
+ * restatement of the reference's arithmetic (citations per function in
+ * oracle.cpp); it is cross-checked against dense numpy/scipy known answers in
+ * tests/test_oracle_kat.py.
+ */
+#ifndef NLSB_ORACLE_H
+#define NLSB_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Integrator ids (same numbering as the product's include/nlsb200.h). */
+enum {
+  ORC_KG_GAUTSCHI = 0,  /* kg_single.cuh:94-126 */
+  ORC_KG_SV = 1,        /* kg_single.cuh:145-178 */
+  ORC_SP4_SV = 2,       /* stochastic_phi4.cuh:19-77 */
+  ORC_SP4_GAUTSCHI = 3, /* Gautschi step with the phi^4 force (build extension) */
+  ORC_NLSE_SS2 = 4,     /* nlse_dev.hpp:187-203 */
+  ORC_NLSE_SEWI = 5     /* nlse_dev.hpp:205-239 */
+};
+
+/* Matrix functions (matfunc_real.hpp:102, matfunc_complex.hpp:269-303). */
+enum {
+  ORC_F_COS_SQRT = 0,   /* cos(t sqrt|lambda|) */
+  ORC_F_SINC2_SQRT = 1, /* (sin x / x)^2, x = t sqrt|lambda|, |x|<1e-8 -> 1 */
+  ORC_F_ID_SQRT = 2,    /* t sqrt|lambda| */
+  ORC_F_EXP = 3,        /* exp(dt * lambda), dt complex */
+  ORC_F_SINC = 4        /* sin(dt lambda)/(dt lambda), |dt lambda|<1e-8 -> 1 */
+};
+
+typedef struct orc_problem {
+  int32_t dim;          /* 2 or 3 */
+  int32_t nx, ny, nz;   /* full grid including the ghost ring (driver argv) */
+  double Lx, Ly, Lz;
+  double T;
+  int32_t nt, ns;
+  int32_t k;            /* Krylov dimension */
+  int32_t method;       /* ORC_* integrator id */
+  int32_t sewi_variant; /* 0: reference operand order, 1: corrected */
+  int32_t reorth;       /* 1: classical Gram-Schmidt pass as lanczos.hpp:249-250 */
+  int32_t max_steps;    /* >0: stop after this many steps (bounded timing sample) */
+  int32_t pad_;
+  /* nonlinearity g(u) = (p1 m + q1) u + (p3 m + q3) u^3 + (rm m + r0) xi   (KG / phi4)
+     NLSE density rho = (p3 m + q3) |u|^2                                           */
+  double p1, q1, p3, q3, rm, r0;
+  uint64_t seed;        /* Philox key for phi4 noise */
+} orc_problem;
+
+/* y = sign * L(c) x on the full grid; L is the no-flux finite-volume operator of
+   laplacians.hpp:54-103 / 158-218 scaled by inv_h2. is_complex: x,y interleaved. */
+void orc_apply_operator(int32_t dim, int32_t nx, int32_t ny, int32_t nz,
+                        double inv_h2, double sign, const double *c,
+                        const double *x, double *y, int32_t is_complex);
+
+/* Symmetric tridiagonal eigendecomposition (implicit QL). diag[n], sub[n]
+   (sub[i] couples i and i+1; sub[n-1] ignored). evecs: n*n column-major. */
+int32_t orc_tridiag_eig(int32_t n, const double *diag, const double *sub,
+                        double *evals, double *evecs);
+
+/* f(T) e1 for the k x k column-major Lanczos matrix T (lower triangle read,
+   as cusolverDn{D,Z}{sy,he}evd with FILL_MODE_LOWER). Complex T/out interleaved. */
+int32_t orc_fT_e1(int32_t k, const double *T, int32_t is_complex, int32_t ftype,
+                  double t_re, double t_im, double *out);
+
+/* out = f(A) in via k-step Lanczos (matfunc_real.hpp:190-313 /
+   matfunc_complex.hpp:254-375). T_out (optional, k*k column-major) receives T. */
+int32_t orc_matfunc(int32_t dim, int32_t nx, int32_t ny, int32_t nz,
+                    double inv_h2, double sign, const double *c, int32_t k,
+                    int32_t is_complex, int32_t ftype, double t_re, double t_im,
+                    int32_t reorth, const double *in, double *out, double *T_out);
+
+/* One standard normal per (seed, step, point): Philox4x32-10 + Box-Muller. */
+double orc_philox_normal(uint64_t seed, uint32_t step, uint32_t point);
+
+/* Raw Philox4x32-10 block (for the Random123 known-answer vectors). */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Full driver run: snapshot 0 = initial state, snapshot s = state after step
+   s*freq (freq = nt/ns). traj/vel: ns*n doubles (complex: interleaved, vel unused).
+   Returns 0 or a negative error. */
+int32_t orc_run(const orc_problem *p, const double *u0, const double *v0,
+                const double *m, const double *c, double *traj, double *vel);
+
+/* Number of OpenMP threads the oracle uses. */
+int32_t orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
