@@ -130,11 +130,17 @@ int nls_pool_set_segment(nls_pool *pool, int32_t rows);
    with CUDA events; *ms = mean duration of one launch; *points = grid points
    covered by one launch. The pass is idempotent, so the state is unchanged. */
 int nls_pool_time_pass(nls_pool *pool, int32_t j, int32_t iters, float *ms, int64_t *points);
-/* Time `iters` whole steps of the pool without advancing trajectories is not
-   possible; steps are timed by the caller around nls_pool_step. */
+/* Advance like nls_pool_step and time the steps with CUDA events recorded on
+   the pool's stream around them (waits for completion): *ms = device time of
+   all nsteps steps. */
+int nls_pool_step_timed(nls_pool *pool, int32_t nsteps, float *ms);
 /* Launch counts of the most recent step: kernels launched per step. */
 int nls_pool_kernels_per_step(nls_pool *pool, int32_t *count);
 int nls_pool_destroy(nls_pool *pool);
+
+/* Select the CUDA device for the calling thread's subsequent pools/handles
+   (one process per GPU; the library keeps its own runtime state). */
+int nls_set_device(int32_t device);
 
 const char *nls_strerror(int code);
 /* Copy the calling thread's last error message (NUL-terminated). */

@@ -583,7 +583,7 @@ int issue_copies(nls_pool *P, SlotHost &h, const SlotDesc &d, int step) {
   return NLS_OK;
 }
 
-int pool_step_once(nls_pool *P) {
+int pool_step_prepare(nls_pool *P) {
   // slots whose step count is exhausted leave the tables
   for (int s = 0; s < P->max_slots; ++s) {
     const bool act = P->hs[s].used && P->hs[s].step <= P->hs[s].nt - 1;
@@ -597,6 +597,12 @@ int pool_step_once(nls_pool *P) {
     int rc = rebuild_tables(P);
     if (rc) return rc;
   }
+  return NLS_OK;
+}
+
+int pool_step_once(nls_pool *P) {
+  int rc0 = pool_step_prepare(P);
+  if (rc0) return rc0;
   if (P->main.nlist == 0 && P->first.nlist == 0) return NLS_OK;
   for (TileSet *T : {&P->first, &P->main})
     for (int s : T->list) {
@@ -699,6 +705,11 @@ const char *nls_strerror(int code) {
   case NLS_ERR_IO: return "I/O error";
   }
   return "unknown error";
+}
+
+int nls_set_device(int32_t device) {
+  CK(cudaSetDevice(device));
+  return NLS_OK;
 }
 
 int nls_last_error(char *buf, int32_t len) {
@@ -931,6 +942,30 @@ int nls_pool_step(nls_pool *P, int32_t nsteps) {
     int rc = pool_step_once(P);
     if (rc) return rc;
   }
+  return NLS_OK;
+}
+
+int nls_pool_step_timed(nls_pool *P, int32_t nsteps, float *ms) {
+  if (!P || !ms) return fail(NLS_ERR_INVALID_ARG, "null");
+  // tables are rebuilt before the first event so that host-side staging is
+  // outside the timed interval
+  int rc = pool_step_prepare(P);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, P->stream));
+  rc = nls_pool_step(P, nsteps);
+  if (rc) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+  }
+  CK(cudaEventRecord(e1, P->stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return NLS_OK;
 }
 

@@ -31,6 +31,7 @@ SYMBOLS = [
     "nls_pool_poll", "nls_pool_release", "nls_pool_sync", "nls_pool_usage",
     "nls_pool_set_graphs", "nls_pool_set_segment", "nls_pool_time_pass",
     "nls_pool_kernels_per_step", "nls_pool_destroy", "nls_strerror", "nls_last_error",
+    "nls_pool_step_timed", "nls_set_device",
 ]
 
 
@@ -96,7 +97,9 @@ def lib() -> ctypes.CDLL:
         "nls_pool_set_segment": [vp, i32],
         "nls_pool_time_pass": [vp, i32, i32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(i64)],
         "nls_pool_kernels_per_step": [vp, ip],
+        "nls_pool_step_timed": [vp, i32, ctypes.POINTER(ctypes.c_float)],
         "nls_pool_destroy": [vp],
+        "nls_set_device": [i32],
         "nls_last_error": [ctypes.c_char_p, i32],
     }
     for name, args in sig.items():

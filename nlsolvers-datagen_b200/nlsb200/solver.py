@@ -213,6 +213,12 @@ class Pool:
     def step(self, nsteps: int = 1):
         check(lib().nls_pool_step(self._p, int(nsteps)))
 
+    def step_timed(self, nsteps: int) -> float:
+        """Advance nsteps steps; device time in ms (CUDA events on the pool stream)."""
+        ms = ctypes.c_float()
+        check(lib().nls_pool_step_timed(self._p, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
     def poll(self, slot: int):
         done, fin = ctypes.c_int32(), ctypes.c_int32()
         check(lib().nls_pool_poll(self._p, slot, ctypes.byref(done), ctypes.byref(fin)))

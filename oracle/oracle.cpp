@@ -381,21 +381,57 @@ inline double force(const orc_problem *p, double u, double m, double xi) {
          (p->rm * m + p->r0) * xi;
 }
 
+// State of a KG / phi4 trajectory between steps (kg_dev.hpp:319-339).
+struct RealState {
+  orc_problem p;
+  Derived D;
+  std::vector<double> u, v, up, buf, buf2, buf3, m, c;
+  int step = 1;
+};
+
+int real_steps(RealState &S, int nsteps, double *traj, double *vel);
+
 // KG / phi4 drivers: kg_driver_dev_2d.cpp:144-153 loop, kg_dev.hpp:55-58 init,
 // KGESolver::step (kg_single.cuh:94-126), step_sv (:145-178),
 // SP4Solver::step (stochastic_phi4.cuh:19-77), BC then snapshot.
+void real_init(RealState &S, const orc_problem *p, const Derived &D, const double *u0,
+               const double *v0, const double *m, const double *c) {
+  const long n = D.g.n;
+  S.p = *p;
+  S.D = D;
+  S.u.assign(u0, u0 + n);
+  S.v.assign(v0, v0 + n);
+  S.up.resize(n);
+  S.buf.resize(n);
+  S.buf2.resize(n);
+  S.buf3.resize(n);
+  S.m.assign(m, m + n);
+  S.c.assign(c, c + n);
+  for (long i = 0; i < n; ++i) S.up[i] = u0[i] - D.dt * v0[i];
+  S.step = 1;
+}
+
 int run_real(const orc_problem *p, const Derived &D, const double *u0, const double *v0,
              const double *m, const double *c, double *traj, double *vel) {
+  RealState S;
+  real_init(S, p, D, u0, v0, m, c);
+  std::copy(S.u.begin(), S.u.end(), traj);
+  std::copy(S.v.begin(), S.v.end(), vel);
+  const int last = p->max_steps > 0 ? std::min(p->nt - 1, p->max_steps) : p->nt - 1;
+  return real_steps(S, last, traj, vel);
+}
+
+int real_steps(RealState &S, int nsteps, double *traj, double *vel) {
+  const orc_problem *p = &S.p;
+  const Derived &D = S.D;
   const long n = D.g.n;
   const double dt = D.dt;
-  std::vector<double> u(u0, u0 + n), v(v0, v0 + n), up(n), buf(n), buf2(n), buf3(n);
-  for (long i = 0; i < n; ++i) up[i] = u0[i] - dt * v0[i];
-  std::copy(u.begin(), u.end(), traj);
-  std::copy(v.begin(), v.end(), vel);
+  std::vector<double> &u = S.u, &v = S.v, &up = S.up, &buf = S.buf, &buf2 = S.buf2, &buf3 = S.buf3;
+  const double *m = S.m.data(), *c = S.c.data();
   const bool gautschi = p->method == ORC_KG_GAUTSCHI || p->method == ORC_SP4_GAUTSCHI;
   const bool noisy = p->rm != 0.0 || p->r0 != 0.0;
-  const int last = p->max_steps > 0 ? std::min(p->nt - 1, p->max_steps) : p->nt - 1;
-  for (int step = 1; step <= last; ++step) {
+  const int last = std::min(p->nt - 1, S.step + nsteps - 1);
+  for (int step = S.step; step <= last; ++step, S.step = step) {
     std::copy(u.begin(), u.end(), buf.begin());
     if (gautschi) {
       int rc = matfunc<double>(D.g, D.inv_h2, -1.0, c, p->k, ORC_F_COS_SQRT, cd(dt, 0.0),
@@ -433,7 +469,7 @@ int run_real(const orc_problem *p, const Derived &D, const double *u0, const dou
     std::copy(buf.begin(), buf.end(), up.begin());
     for (long i = 0; i < n; ++i) v[i] = (u[i] - up[i]) / dt;
     apply_bc(D.g, u.data());
-    if (step % D.freq == 0) {
+    if (traj && step % D.freq == 0) {
       const int s = step / D.freq;
       if (s < p->ns) {
         std::copy(u.begin(), u.end(), traj + (size_t)s * n);
@@ -441,6 +477,7 @@ int run_real(const orc_problem *p, const Derived &D, const double *u0, const dou
       }
     }
   }
+  S.step = last + 1;
   return 0;
 }
 
@@ -602,6 +639,25 @@ int32_t orc_run(const orc_problem *p, const double *u0, const double *v0, const 
   }
   return -1;
 }
+
+void *orc_real_begin(const orc_problem *p, const double *u0, const double *v0, const double *m,
+                     const double *c) {
+  Derived D;
+  if (derive(p, D) != 0 || p->method == ORC_NLSE_SS2 || p->method == ORC_NLSE_SEWI) return nullptr;
+  RealState *S = new RealState();
+  real_init(*S, p, D, u0, v0, m, c);
+  return S;
+}
+
+int32_t orc_real_advance(void *state, int32_t nsteps, double *u_out) {
+  RealState *S = static_cast<RealState *>(state);
+  if (!S) return -1;
+  const int rc = real_steps(*S, nsteps, nullptr, nullptr);
+  if (u_out) std::copy(S->u.begin(), S->u.end(), u_out);
+  return rc;
+}
+
+void orc_real_end(void *state) { delete static_cast<RealState *>(state); }
 
 int32_t orc_num_threads(void) {
 #ifdef _OPENMP

@@ -94,6 +94,14 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 int32_t orc_run(const orc_problem *p, const double *u0, const double *v0,
                 const double *m, const double *c, double *traj, double *vel);
 
+/* Stateful KG / phi4 stepping (for timing pure steps without per-call setup):
+   begin copies the inputs, advance runs nsteps driver-loop steps (step + ghost
+   copies) and optionally copies u out, end frees. */
+void *orc_real_begin(const orc_problem *p, const double *u0, const double *v0, const double *m,
+                     const double *c);
+int32_t orc_real_advance(void *state, int32_t nsteps, double *u_out);
+void orc_real_end(void *state);
+
 /* Number of OpenMP threads the oracle uses. */
 int32_t orc_num_threads(void);
 

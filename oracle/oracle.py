@@ -70,6 +70,12 @@ def lib():
         L.orc_run.argtypes = [ctypes.POINTER(_Problem), dp, dp, dp, dp, dp, dp]
         L.orc_run.restype = ctypes.c_int32
         L.orc_num_threads.restype = ctypes.c_int32
+        L.orc_real_begin.argtypes = [ctypes.POINTER(_Problem), dp, dp, dp, dp]
+        L.orc_real_begin.restype = ctypes.c_void_p
+        L.orc_real_advance.argtypes = [ctypes.c_void_p, ctypes.c_int32, dp]
+        L.orc_real_advance.restype = ctypes.c_int32
+        L.orc_real_end.argtypes = [ctypes.c_void_p]
+        L.orc_real_end.restype = None
         _lib = L
     return _lib
 
@@ -198,6 +204,35 @@ def run(prob: Problem, u0, v0, m, c):
     if rc != 0:
         raise RuntimeError(f"oracle run failed: {rc}")
     return traj, (None if cplx else vel)
+
+
+class RealStepper:
+    """Stateful KG / phi4 oracle trajectory (pure step timing)."""
+
+    def __init__(self, prob: Problem, u0, v0, m, c):
+        shape = (prob.nz, prob.ny, prob.nx) if prob.dim == 3 else (prob.ny, prob.nx)
+        self._arrs = [_f64(np.reshape(a, shape)) for a in
+                      (u0, np.zeros(shape) if v0 is None else v0, m, c)]
+        self._s = prob.struct()
+        self._h = lib().orc_real_begin(ctypes.byref(self._s), *[_p(a) for a in self._arrs])
+        if not self._h:
+            raise RuntimeError("orc_real_begin failed")
+        self.shape = shape
+
+    def advance(self, nsteps, want_u=False):
+        u = np.empty(self.shape) if want_u else None
+        rc = lib().orc_real_advance(self._h, nsteps, _p(u) if want_u else None)
+        if rc != 0:
+            raise RuntimeError(f"oracle advance failed: {rc}")
+        return u
+
+    def close(self):
+        if self._h:
+            lib().orc_real_end(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def num_threads():
