@@ -258,8 +258,10 @@ def run_ours(args, ws, rank, lrank):
     k = None
     kreport = {}
     if rank == 0:
+        # the reference leaves T[k-1,k-1] = 0, so its result converges only
+        # algebraically in k; accept k when 10 probe steps stay within 5e-6 of k = 24
         k, kreport = autotune.choose_k(*probe, candidates=tuple(range(8, 17)), k_ref=24,
-                                       steps=10, tol=1e-9)
+                                       steps=10, tol=5e-6)
     k = bcast_int(k if k is not None else 0, ws)
     cases = make_batch(B, rank, k)
     n = cases[0][0].n

@@ -72,12 +72,34 @@ template <typename K> cudaError_t set_smem(K kernel, size_t bytes) {
 }
 
 // ------------------------------------------------------------ kernel sets
+using LaunchFn = cudaError_t (*)(const StepArgs &, int, cudaStream_t);
 struct Launch {
-  // tile kernels take grid = tiles capacity; others compute their own grid
-  cudaError_t (*first)(const StepArgs &, int, cudaStream_t) = nullptr;
-  cudaError_t (*lanczos)(const StepArgs &, int, cudaStream_t) = nullptr;
-  cudaError_t (*final_)(const StepArgs &, int, cudaStream_t) = nullptr;
+  // [has_c]; tile kernels take grid = tile capacity (3-D: blocks, 2-D: warps)
+  LaunchFn first[2] = {nullptr, nullptr};
+  LaunchFn lanczos[2] = {nullptr, nullptr};
+  LaunchFn final_[2] = {nullptr, nullptr};
 };
+
+template <typename E, int SRC, bool HC>
+cudaError_t launch2_first(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_first<E, SRC, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template <typename E, int NSEQ, bool HC>
+cudaError_t launch2_lanczos(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_lanczos<E, NSEQ, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template <typename E, int NSEQ, int FIN, bool HC>
+cudaError_t launch2_final(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_final<E, NSEQ, FIN, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template <typename R, bool HC>
+cudaError_t launch2_sv(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_sv<R, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
 
 template <int DIM, typename E, int NSEQ, int SRC>
 cudaError_t launch_first(const StepArgs &a, int grid, cudaStream_t st) {
@@ -116,7 +138,7 @@ cudaError_t launch_advance(const StepArgs &a, int nslots_cap, cudaStream_t st) {
 // Kernel table of one (method family, dim, precision).
 struct KSet {
   Launch kg, ss2, sewi_a, sewi_b;  // Gautschi / NLSE phases
-  cudaError_t (*sv)(const StepArgs &, int, cudaStream_t) = nullptr;
+  LaunchFn sv[2] = {nullptr, nullptr};
   cudaError_t (*ftri)(const StepArgs &, int, cudaStream_t) = nullptr;
   cudaError_t (*ring)(const StepArgs &, int, int, cudaStream_t) = nullptr;
   cudaError_t (*set_attrs)() = nullptr;
@@ -142,43 +164,86 @@ template <int DIM, typename E> cudaError_t attrs_cplx() {
   if ((e = set_smem(k_final<DIM, E, 1, FIN_SEWI_B>, smem_final<DIM, E, 1>()))) return e;
   return cudaSuccess;
 }
+cudaError_t attrs_none() { return cudaSuccess; }
 
-template <int DIM, typename R> KSet make_real() {
+// 3-D: shared-memory plane kernels (c handled at run time)
+template <typename R> KSet make_real3() {
   KSet k;
-  k.kg.first = launch_first<DIM, R, 2, SRC_KG>;
-  k.kg.lanczos = launch_lanczos<DIM, R, 2>;
-  k.kg.final_ = launch_final<DIM, R, 2, FIN_KG>;
-  k.sv = launch_sv<DIM, R>;
+  k.kg.first[0] = k.kg.first[1] = launch_first<3, R, 2, SRC_KG>;
+  k.kg.lanczos[0] = k.kg.lanczos[1] = launch_lanczos<3, R, 2>;
+  k.kg.final_[0] = k.kg.final_[1] = launch_final<3, R, 2, FIN_KG>;
+  k.sv[0] = k.sv[1] = launch_sv<3, R>;
   k.ftri = launch_ftri<R>;
   k.ring = launch_ring<R, 0>;
-  k.set_attrs = attrs_real<DIM, R>;
+  k.set_attrs = attrs_real<3, R>;
   return k;
 }
-template <int DIM, typename E> KSet make_cplx() {
+template <typename E> KSet make_cplx3() {
   KSet k;
-  k.ss2.first = launch_first<DIM, E, 1, SRC_SS2>;
-  k.ss2.lanczos = launch_lanczos<DIM, E, 1>;
-  k.ss2.final_ = launch_final<DIM, E, 1, FIN_SS2>;
-  k.sewi_a.first = launch_first<DIM, E, 2, SRC_SEWI_A>;
-  k.sewi_a.lanczos = launch_lanczos<DIM, E, 2>;
-  k.sewi_a.final_ = launch_final<DIM, E, 2, FIN_SEWI_A>;
-  k.sewi_b.first = launch_first<DIM, E, 1, SRC_SEWI_B>;
-  k.sewi_b.lanczos = launch_lanczos<DIM, E, 1>;
-  k.sewi_b.final_ = launch_final<DIM, E, 1, FIN_SEWI_B>;
+  k.ss2.first[0] = k.ss2.first[1] = launch_first<3, E, 1, SRC_SS2>;
+  k.ss2.lanczos[0] = k.ss2.lanczos[1] = launch_lanczos<3, E, 1>;
+  k.ss2.final_[0] = k.ss2.final_[1] = launch_final<3, E, 1, FIN_SS2>;
+  k.sewi_a.first[0] = k.sewi_a.first[1] = launch_first<3, E, 2, SRC_SEWI_A>;
+  k.sewi_a.lanczos[0] = k.sewi_a.lanczos[1] = launch_lanczos<3, E, 2>;
+  k.sewi_a.final_[0] = k.sewi_a.final_[1] = launch_final<3, E, 2, FIN_SEWI_A>;
+  k.sewi_b.first[0] = k.sewi_b.first[1] = launch_first<3, E, 1, SRC_SEWI_B>;
+  k.sewi_b.lanczos[0] = k.sewi_b.lanczos[1] = launch_lanczos<3, E, 1>;
+  k.sewi_b.final_[0] = k.sewi_b.final_[1] = launch_final<3, E, 1, FIN_SEWI_B>;
   k.ftri = launch_ftri<E>;
   k.ring = launch_ring<E, 1>;
-  k.set_attrs = attrs_cplx<DIM, E>;
+  k.set_attrs = attrs_cplx<3, E>;
+  return k;
+}
+// 2-D: warp-marching register kernels, c-field variant chosen per step
+template <typename R> KSet make_real2() {
+  KSet k;
+  k.kg.first[0] = launch2_first<R, SRC_KG, false>;
+  k.kg.first[1] = launch2_first<R, SRC_KG, true>;
+  k.kg.lanczos[0] = launch2_lanczos<R, 2, false>;
+  k.kg.lanczos[1] = launch2_lanczos<R, 2, true>;
+  k.kg.final_[0] = launch2_final<R, 2, FIN_KG, false>;
+  k.kg.final_[1] = launch2_final<R, 2, FIN_KG, true>;
+  k.sv[0] = launch2_sv<R, false>;
+  k.sv[1] = launch2_sv<R, true>;
+  k.ftri = launch_ftri<R>;
+  k.ring = launch_ring<R, 0>;
+  k.set_attrs = attrs_none;
+  return k;
+}
+template <typename E> KSet make_cplx2() {
+  KSet k;
+  k.ss2.first[0] = launch2_first<E, SRC_SS2, false>;
+  k.ss2.first[1] = launch2_first<E, SRC_SS2, true>;
+  k.ss2.lanczos[0] = launch2_lanczos<E, 1, false>;
+  k.ss2.lanczos[1] = launch2_lanczos<E, 1, true>;
+  k.ss2.final_[0] = launch2_final<E, 1, FIN_SS2, false>;
+  k.ss2.final_[1] = launch2_final<E, 1, FIN_SS2, true>;
+  k.sewi_a.first[0] = launch2_first<E, SRC_SEWI_A, false>;
+  k.sewi_a.first[1] = launch2_first<E, SRC_SEWI_A, true>;
+  k.sewi_a.lanczos[0] = launch2_lanczos<E, 2, false>;
+  k.sewi_a.lanczos[1] = launch2_lanczos<E, 2, true>;
+  k.sewi_a.final_[0] = launch2_final<E, 2, FIN_SEWI_A, false>;
+  k.sewi_a.final_[1] = launch2_final<E, 2, FIN_SEWI_A, true>;
+  k.sewi_b.first[0] = launch2_first<E, SRC_SEWI_B, false>;
+  k.sewi_b.first[1] = launch2_first<E, SRC_SEWI_B, true>;
+  k.sewi_b.lanczos[0] = launch2_lanczos<E, 1, false>;
+  k.sewi_b.lanczos[1] = launch2_lanczos<E, 1, true>;
+  k.sewi_b.final_[0] = launch2_final<E, 1, FIN_SEWI_B, false>;
+  k.sewi_b.final_[1] = launch2_final<E, 1, FIN_SEWI_B, true>;
+  k.ftri = launch_ftri<E>;
+  k.ring = launch_ring<E, 1>;
+  k.set_attrs = attrs_none;
   return k;
 }
 
 KSet kset_for(int method, int dim, int prec) {
   const bool cplx = method == NLS_NLSE_SS2 || method == NLS_NLSE_SEWI;
   if (!cplx) {
-    if (dim == 2) return prec == NLS_FP64 ? make_real<2, double>() : make_real<2, float>();
-    return prec == NLS_FP64 ? make_real<3, double>() : make_real<3, float>();
+    if (dim == 2) return prec == NLS_FP64 ? make_real2<double>() : make_real2<float>();
+    return prec == NLS_FP64 ? make_real3<double>() : make_real3<float>();
   }
-  if (dim == 2) return prec == NLS_FP64 ? make_cplx<2, Cx<double>>() : make_cplx<2, Cx<float>>();
-  return prec == NLS_FP64 ? make_cplx<3, Cx<double>>() : make_cplx<3, Cx<float>>();
+  if (dim == 2) return prec == NLS_FP64 ? make_cplx2<Cx<double>>() : make_cplx2<Cx<float>>();
+  return prec == NLS_FP64 ? make_cplx3<Cx<double>>() : make_cplx3<Cx<float>>();
 }
 
 bool is_cplx(int method) { return method == NLS_NLSE_SS2 || method == NLS_NLSE_SEWI; }
@@ -272,6 +337,7 @@ struct nls_pool {
   LzScal *d_scal = nullptr;
   double *d_beta0 = nullptr;
   FinalCoef *d_coef = nullptr;
+  int *d_ticket = nullptr;
   TileSet main, first;  // main step / SEWI Strang first steps
   std::vector<SlotHost> hs;
   std::vector<SlotDesc> sd;
@@ -281,7 +347,9 @@ struct nls_pool {
   cudaEvent_t ev_step = nullptr;
   bool use_graph = true;
   cudaGraphExec_t gexec = nullptr;
-  int graph_tiles = -1, graph_ring = -1;
+  int graph_tiles = -1, graph_ring = -1, graph_hc = -1;
+  void *graph_part = nullptr;
+  int step_hc = 0;  // some stepped slot carries a c field
   int ring_blocks = 1;
   int kernels_per_step = 0;
   int device = 0;
@@ -322,7 +390,7 @@ int check_problem(const nls_problem *p) {
 void pool_free_device(nls_pool *P) {
   void *bufs[] = {P->u_hi, P->u_lo, P->u_alt, P->d, P->up_hi, P->up_lo, P->ya, P->ib, P->m,
                   P->c,    P->V,    P->snap,  P->part, P->d_slots, P->d_state, P->d_scal,
-                  P->d_beta0, P->d_coef, P->main.d_tiles, P->main.d_ntiles, P->main.d_list,
+                  P->d_beta0, P->d_coef, P->d_ticket, P->main.d_tiles, P->main.d_ntiles, P->main.d_list,
                   P->main.d_nlist, P->first.d_tiles, P->first.d_ntiles, P->first.d_list,
                   P->first.d_nlist};
   for (void *b : bufs)
@@ -335,23 +403,39 @@ int64_t slot_padded(const nls_problem &p, int32_t &pitch) {
   return (np + 255) / 256 * 256;
 }
 
-// Tiles of one slot: 2-D: 128-wide column strips x seg rows; 3-D: 32x8 columns x seg planes.
+// Tiles of one slot. 2-D: warp strips of W <= 30 output vectors (16 bytes each)
+// x seg rows; 3-D: 32x8 columns x seg planes. The tiling depends only on the
+// slot, so its reduction order is the same alone and in any batch.
 void slot_tiles(const nls_pool *P, int slot, const SlotDesc &s, std::vector<TileDesc> &out) {
-  const int tx = P->dim == 2 ? Geo<2>::TX : Geo<3>::TX;
-  const int ty = P->dim == 2 ? 1 : Geo<3>::TY;
-  const int np = P->dim == 2 ? s.ny : s.nz;
-  const int ny = P->dim == 2 ? 1 : s.ny;
-  const int seg = P->dim == 2 ? P->seg2 : P->seg3;
   int local = 0;
-  for (int p0 = 0; p0 < np; p0 += seg)
-    for (int y0 = 0; y0 < ny; y0 += ty)
+  if (P->dim == 2) {
+    const int N = (int)(16 / P->esz);
+    const int nvec = (s.nx + N - 1) / N;
+    const int nseg = (nvec + 29) / 30;
+    const int W = (nvec + nseg - 1) / nseg;
+    for (int p0 = 0; p0 < s.ny; p0 += P->seg2)
+      for (int g = 0; g < nseg; ++g) {
+        TileDesc t;
+        t.slot = slot;
+        t.x0 = g * W * N;
+        t.y0 = std::min(W, nvec - g * W);
+        t.p0 = p0;
+        t.p1 = std::min(s.ny, p0 + P->seg2);
+        t.local = local++;
+        out.push_back(t);
+      }
+    return;
+  }
+  const int tx = Geo<3>::TX, ty = Geo<3>::TY;
+  for (int p0 = 0; p0 < s.nz; p0 += P->seg3)
+    for (int y0 = 0; y0 < s.ny; y0 += ty)
       for (int x0 = 0; x0 < s.nx; x0 += tx) {
         TileDesc t;
         t.slot = slot;
         t.x0 = x0;
         t.y0 = y0;
         t.p0 = p0;
-        t.p1 = std::min(np, p0 + seg);
+        t.p1 = std::min(s.nz, p0 + P->seg3);
         t.local = local++;
         out.push_back(t);
       }
@@ -387,6 +471,7 @@ int rebuild_tables(nls_pool *P) {
   P->main.list.clear();
   P->first.tiles.clear();
   P->first.list.clear();
+  P->step_hc = 0;
   int max_ring = 1;
   for (int s = 0; s < P->max_slots; ++s) {
     SlotHost &h = P->hs[s];
@@ -399,6 +484,7 @@ int rebuild_tables(nls_pool *P) {
     d.tile_count = (int)T.tiles.size() - d.tile_begin;
     T.list.push_back(s);
     max_ring = std::max(max_ring, h.ring_cnt);
+    if (d.has_c) P->step_hc = 1;
   }
   int rb = 1;
   while (rb * 256 * 4 < max_ring && rb < 256) rb *= 2;
@@ -451,22 +537,25 @@ StepArgs base_args(const nls_pool *P, const TileSet &T) {
   a.scal = P->d_scal;
   a.beta0 = P->d_beta0;
   a.coef = P->d_coef;
+  a.ticket = P->d_ticket;
+  a.scal_ready = P->dim == 2 ? 1 : 0;
+  a.has_c = P->step_hc;
   return a;
 }
 
 // One Krylov application family (first pass, Lanczos passes, f(T), final).
 int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &nk) {
-  const int grid = T.cap;
-  CK(L.first(a, grid, P->stream));
+  const int grid = T.cap, hc = P->step_hc;
+  CK(L.first[hc](a, grid, P->stream));
   ++nk;
   for (int j = 1; j <= P->k - 2; ++j) {
     a.j = j;
-    CK(L.lanczos(a, grid, P->stream));
+    CK(L.lanczos[hc](a, grid, P->stream));
     ++nk;
   }
   CK(P->ks.ftri(a, P->max_slots, P->stream));
   ++nk;
-  CK(L.final_(a, grid, P->stream));
+  CK(L.final_[hc](a, grid, P->stream));
   ++nk;
   return NLS_OK;
 }
@@ -478,7 +567,7 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
   const int m = P->method;
   if (is_sv(m)) {
     a.sv_pingpong = 1;
-    CK(P->ks.sv(a, T.cap, P->stream));
+    CK(P->ks.sv[P->step_hc](a, T.cap, P->stream));
     ++nk;
   } else if (m == NLS_KG_GAUTSCHI || m == NLS_SP4_GAUTSCHI) {
     // kg_single.cuh:103-111: cos(tau sqrt A) u and sinc^2(tau sqrt A) g(u), A = -L
@@ -533,7 +622,8 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
 
 int run_main_step(nls_pool *P) {
   if (!P->use_graph) return enqueue_step(P, P->main, false);
-  if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks) {
+  if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks ||
+      P->graph_hc != P->step_hc || P->graph_part != (void *)P->part) {
     if (P->gexec) {
       cudaGraphExecDestroy(P->gexec);
       P->gexec = nullptr;
@@ -552,6 +642,8 @@ int run_main_step(nls_pool *P) {
     CK(e3);
     P->graph_tiles = P->main.cap;
     P->graph_ring = P->ring_blocks;
+    P->graph_hc = P->step_hc;
+    P->graph_part = (void *)P->part;
   }
   CK(cudaGraphLaunch(P->gexec, P->stream));
   return NLS_OK;
@@ -661,7 +753,7 @@ int upload_slot(nls_pool *P, int s, const double *u0, const double *v0, const do
           put(lo, e, q, u - uh, false);
         }
         put(mr, e, 0, m[pt], true);
-        if (p.has_c) put(cr, e, 0, c[pt], true);
+        put(cr, e, 0, p.has_c ? c[pt] : 1.0, true);
         if (!P->cplx) {
           // u_past = u0 - dt v0 (kg_dev.hpp:55-58); d = u0 - u_past
           const double vv = v0 ? v0[pt] : 0.0;
@@ -673,7 +765,7 @@ int upload_slot(nls_pool *P, int s, const double *u0, const double *v0, const do
   CK(cudaMemcpyAsync((char *)P->u_hi + eo * P->esz, hi.data(), np * P->esz, cudaMemcpyHostToDevice, P->stream));
   CK(cudaMemcpyAsync((char *)P->u_lo + eo * P->esz, lo.data(), np * P->esz, cudaMemcpyHostToDevice, P->stream));
   CK(cudaMemcpyAsync((char *)P->m + eo * P->rsz, mr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
-  if (p.has_c) CK(cudaMemcpyAsync((char *)P->c + eo * P->rsz, cr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
+  CK(cudaMemcpyAsync((char *)P->c + eo * P->rsz, cr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
   if (!P->cplx) CK(cudaMemcpyAsync((char *)P->d + eo * P->rsz, dd.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
   if (P->method == NLS_NLSE_SEWI) {
     // u_prev <- u0 before the first (Strang) step (nlse_dev.hpp:206-209)
@@ -808,6 +900,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_scal, sizeof(LzScal) * max_slots * 2 * KMAX);
   if (!rc) rc = al((void **)&P->d_beta0, sizeof(double) * max_slots * 2);
   if (!rc) rc = al((void **)&P->d_coef, sizeof(FinalCoef) * max_slots * 2);
+  if (!rc) rc = al((void **)&P->d_ticket, sizeof(int) * max_slots);
   for (TileSet *T : {&P->main, &P->first}) {
     if (!rc) rc = al((void **)&T->d_ntiles, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlist, sizeof(int));
@@ -824,6 +917,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
     cudaError_t e = cudaMemsetAsync(P->d_state, 0, sizeof(SlotState) * max_slots, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->snap, 0, sizeof(double) * ce * 2 * NF, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->d_coef, 0, sizeof(FinalCoef) * max_slots * 2, P->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->d_ticket, 0, sizeof(int) * max_slots, P->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
     if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -1069,9 +1163,10 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  CK(L.lanczos(a, P->main.cap, P->stream));  // warm
+  const int hc = P->step_hc;
+  CK(L.lanczos[hc](a, P->main.cap, P->stream));  // warm
   CK(cudaEventRecord(e0, P->stream));
-  for (int i = 0; i < iters; ++i) CK(L.lanczos(a, P->main.cap, P->stream));
+  for (int i = 0; i < iters; ++i) CK(L.lanczos[hc](a, P->main.cap, P->stream));
   CK(cudaEventRecord(e1, P->stream));
   CK(cudaEventSynchronize(e1));
   float t = 0.f;

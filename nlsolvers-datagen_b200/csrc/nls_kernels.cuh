@@ -61,6 +61,8 @@ struct StepArgs {
   double tsc[2][2];      // (re, im) time argument per sequence, in units of the slot's dt
   int has_c;             // any slot with a c field
   int sv_pingpong;       // SV step: u_hi / u_alt alternate by step parity
+  int *ticket;           // [slot] arrival counters of the 2-D passes
+  int scal_ready;        // 1: every pass published its scalars (2-D path)
 };
 
 template <int DIM> struct Geo {
@@ -482,10 +484,11 @@ __device__ inline void fval(int fk, double lam, double tr, double ti, double &fr
   }
 }
 
-// One warp per (slot, sequence). Lane r owns row r of the eigenvector matrix.
-// The tridiagonal recurrences of the implicit QL method (Bowdler, Martin,
-// Reinsch & Wilkinson 1968) run redundantly in every lane; the rotations of
-// the eigenvector rows run in parallel across lanes.
+// One warp per (slot, sequence). Lane 0 runs the scalar recurrences of the
+// implicit QL method (Bowdler, Martin, Reinsch & Wilkinson 1968) and records
+// the Givens rotations of each sweep; after every sweep all lanes apply them
+// to their own row of the eigenvector matrix. Iterations per eigenvalue are
+// capped (60); a slot that does not converge gets status NLS_ERR_NUMERIC.
 template <typename E>
 __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   constexpr bool CP = Traits<E>::cplx;
@@ -496,26 +499,30 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   const int li = gw / a.nseq, sq = gw % a.nseq;
   __shared__ double Zs[4][KMAX * (KMAX + 1)];
   __shared__ double dS[4][KMAX], eS[4][KMAX], dl_r[4][KMAX], dl_i[4][KMAX];
+  __shared__ double rcS[4][KMAX], rsS[4][KMAX], fS[4][KMAX][2];
   if (li >= *a.nslot_list) return;
   const int slot = a.slot_list[li];
   const SlotDesc &s = a.slots[slot];
   const int k = a.k, jl = k - 2;
   constexpr int ND = CP ? 9 : 6;
-  const int NV = ND * a.nseq;
-  // last pass scalars
-  double tot = 0.0;
-  if (lane < ND) {
-    const double *pp = a.part + (long long)jl * a.part_stride;
-    for (int t = 0; t < s.tile_count; ++t) tot += pp[(long long)(s.tile_begin + t) * NV + sq * ND + lane];
-  }
-  double tv[9];
+  LzScal Lk;
+  if (a.scal_ready) {
+    Lk = a.scal[(slot * 2 + sq) * KMAX + jl];
+  } else {
+    const int NV = ND * a.nseq;
+    double tot = 0.0;
+    if (lane < ND) {
+      const double *pp = a.part + (long long)jl * a.part_stride;
+      for (int t = 0; t < s.tile_count; ++t) tot += pp[(long long)(s.tile_begin + t) * NV + sq * ND + lane];
+    }
+    double tv[9];
 #pragma unroll
-  for (int q = 0; q < 9; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
-  const LzScal Ll = lz_from_dots<CP>(tv, Eps<R>::v);
-  double *d = dS[wib], *e = eS[wib], *Z = Zs[wib];
+    for (int q = 0; q < 9; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    Lk = lz_from_dots<CP>(tv, Eps<R>::v);
+  }
+  double *d = dS[wib], *e = eS[wib], *Z = Zs[wib], *rc = rcS[wib], *rs = rsS[wib];
   const int ZS = KMAX + 1;
   const double beta0 = a.beta0[slot * 2 + sq];
-  LzScal Lk = Ll;
   if (lane == 0) {
     // T: diag alpha_0..alpha_{k-2}, 0 (lanczos.hpp:217,234); lower subdiagonal
     // T[j, j-1] = d_j (j = 1..k-2, lanczos.hpp:238-239), T[k-1, k-2] = b_{k-1}.
@@ -554,80 +561,90 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   __syncwarp();
   if (lane < k) Z[lane * ZS + lane] = 1.0;
   __syncwarp();
-  // implicit QL; all lanes execute the scalar recurrence on shared d, e
   int status = 0;
-  for (int l = 0; l < k; ++l) {
-    int iter = 0;
-    for (;;) {
-      int m = l;
-      for (; m < k - 1; ++m) {
-        const double dd = fabs(d[m]) + fabs(d[m + 1]);
-        if (fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
-      }
-      if (m == l) break;
-      if (++iter > 60) {
-        status = -1;
-        break;
-      }
-      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double r = hypot(g, 1.0);
-      g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
-      double sn = 1.0, cs = 1.0, p = 0.0;
-      bool defl = false;
-      for (int i = m - 1; i >= l; --i) {
-        const double f = sn * e[i];
-        const double b = cs * e[i];
-        r = hypot(f, g);
-        __syncwarp();
-        if (lane == 0) e[i + 1] = r;
-        __syncwarp();
-        if (r == 0.0) {
-          if (lane == 0) {
-            d[i + 1] -= p;
+  for (int l = 0; l < k && !status; ++l) {
+    for (int iter = 0;; ++iter) {
+      int m = l, nrot = 0, done = 0;
+      if (lane == 0) {
+        for (; m < k - 1; ++m) {
+          const double dd = fabs(d[m]) + fabs(d[m + 1]);
+          if (fabs(e[m]) <= 2.220446049250313e-16 * dd) break;
+        }
+        if (m == l) {
+          done = 1;
+        } else if (iter >= 60) {
+          done = 1;
+          status = -1;
+        } else {
+          double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+          double r = sqrt(g * g + 1.0);
+          g = d[m] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+          double sn = 1.0, cs = 1.0, p = 0.0;
+          bool defl = false;
+          for (int i = m - 1; i >= l; --i) {
+            const double f = sn * e[i];
+            const double b = cs * e[i];
+            const double t2 = f * f + g * g;
+            if (t2 == 0.0) {
+              e[i + 1] = 0.0;
+              d[i + 1] -= p;
+              e[m] = 0.0;
+              defl = true;
+              break;
+            }
+            const double ir = rsqrt(t2);
+            r = t2 * ir;
+            e[i + 1] = r;
+            sn = f * ir;
+            cs = g * ir;
+            g = d[i + 1] - p;
+            r = (d[i] - g) * sn + 2.0 * cs * b;
+            p = sn * r;
+            d[i + 1] = g + p;
+            g = cs * r - b;
+            rc[nrot] = cs;
+            rs[nrot] = sn;
+            ++nrot;
+          }
+          if (!defl) {
+            d[l] -= p;
+            e[l] = g;
             e[m] = 0.0;
           }
-          __syncwarp();
-          defl = true;
-          break;
         }
-        sn = f / r;
-        cs = g / r;
-        g = d[i + 1] - p;
-        r = (d[i] - g) * sn + 2.0 * cs * b;
-        p = sn * r;
-        __syncwarp();
-        if (lane == 0) d[i + 1] = g + p;
-        __syncwarp();
-        g = cs * r - b;
-        if (lane < k) {  // rotate columns i, i+1 of row `lane`
+      }
+      m = __shfl_sync(0xffffffffu, m, 0);
+      nrot = __shfl_sync(0xffffffffu, nrot, 0);
+      done = __shfl_sync(0xffffffffu, done, 0);
+      status = __shfl_sync(0xffffffffu, status, 0);
+      __syncwarp();
+      if (lane < k) {  // rotate columns i, i+1 of row `lane`, i = m-1 .. m-nrot
+        for (int q = 0; q < nrot; ++q) {
+          const int i = m - 1 - q;
           const double zi = Z[lane * ZS + i], zi1 = Z[lane * ZS + i + 1];
-          Z[lane * ZS + i + 1] = sn * zi + cs * zi1;
-          Z[lane * ZS + i] = cs * zi - sn * zi1;
+          Z[lane * ZS + i + 1] = rs[q] * zi + rc[q] * zi1;
+          Z[lane * ZS + i] = rc[q] * zi - rs[q] * zi1;
         }
       }
-      if (status) break;
-      if (defl) continue;
       __syncwarp();
-      if (lane == 0) {
-        d[l] -= p;
-        e[l] = g;
-        e[m] = 0.0;
-      }
-      __syncwarp();
+      if (done) break;
     }
-    if (status) break;
   }
-  __syncwarp();
-  // c_r = delta_r sum_i f(lambda_i) Z[0][i] Z[r][i]
-  double cr = 0.0, ci = 0.0;
+  // f(lambda_i) in parallel, then c_r = delta_r sum_i f(lambda_i) Z[0][i] Z[r][i]
   const int fk = a.fkind[sq];
   if (lane < k) {
+    double fr, fi;
+    fval(fk, d[lane], a.tsc[sq][0] * s.dt, a.tsc[sq][1] * s.dt, fr, fi);
+    fS[wib][lane][0] = fr * Z[0 * ZS + lane];
+    fS[wib][lane][1] = fi * Z[0 * ZS + lane];
+  }
+  __syncwarp();
+  double cr = 0.0, ci = 0.0;
+  if (lane < k) {
     for (int i = 0; i < k; ++i) {
-      double fr, fi;
-      fval(fk, d[i], a.tsc[sq][0] * s.dt, a.tsc[sq][1] * s.dt, fr, fi);
-      const double w = Z[0 * ZS + i] * Z[lane * ZS + i];
-      cr += fr * w;
-      ci += fi * w;
+      const double z = Z[lane * ZS + i];
+      cr += fS[wib][i][0] * z;
+      ci += fS[wib][i][1] * z;
     }
     const double dr = dl_r[wib][lane], di = dl_i[wib][lane];
     const double tr = dr * cr - di * ci, ti = dr * ci + di * cr;
@@ -638,19 +655,17 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   // coefficients of the final combination
   FinalCoef &F = a.coef[slot * 2 + sq];
   const double s0 = beta0 > 0.0 ? 1.0 / beta0 : 0.0;
-  const double sA = (jl == 0) ? s0 : 1.0;          // scale of V_{k-2}
-  const double sB = (jl - 1 == 0) ? s0 : 1.0;      // scale of V_{k-3}
-  // w_j = beta0 c_j s_j (s_0 = 1/beta0)
+  const double sA = (jl == 0) ? s0 : 1.0;      // scale of V_{k-2}
+  const double sB = (jl - 1 == 0) ? s0 : 1.0;  // scale of V_{k-3}
   double wr = 0.0, wi = 0.0;
   if (lane < k - 1) {
     const double sj = lane == 0 ? s0 : 1.0;
     wr = beta0 * sj * cr;
     wi = beta0 * sj * ci;
   }
-  // lam = beta0 c_{k-1} inv_b_{k-1}
+  // lam = beta0 c_{k-1} inv_b_{k-1}; y += lam (sA A V_{k-2} - d sB V_{k-3} - a sA V_{k-2})
   const double lr = __shfl_sync(0xffffffffu, cr, k - 1) * beta0 * Lk.inv_b;
   const double lim = __shfl_sync(0xffffffffu, ci, k - 1) * beta0 * Lk.inv_b;
-  // y += lam (sA A V_{k-2} - d sB V_{k-3} - alpha sA V_{k-2})
   if (lane == k - 2) {
     wr -= sA * (lr * Lk.ar - lim * Lk.ai);
     wi -= sA * (lr * Lk.ai + lim * Lk.ar);
@@ -662,10 +677,14 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   if (lane < k - 1) {
     F.wr[lane] = wr;
     F.wi[lane] = wi;
+    F.wr32[lane] = (float)wr;
+    F.wi32[lane] = (float)wi;
   }
   if (lane == 0) {
     F.lam_r = lr * sA;
     F.lam_i = lim * sA;
+    F.lam32[0] = (float)(lr * sA);
+    F.lam32[1] = (float)(lim * sA);
     F.beta0 = beta0;
     F.kv = k - 1;
     a.scal[(slot * 2 + sq) * KMAX + jl] = Lk;
@@ -674,5 +693,6 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
 }
 
 #include "nls_kernels_tail.cuh"
+#include "nls_warp2d.cuh"
 
 }  // namespace nlsb

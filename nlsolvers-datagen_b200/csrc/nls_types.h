@@ -56,6 +56,8 @@ struct FinalCoef {
   double beta0;
   int32_t kv;  // number of stored vectors (k - 1)
   int32_t pad_;
+  float wr32[KMAX], wi32[KMAX];  // the same coefficients rounded for FP32 slots
+  float lam32[2];
 };
 
 }  // namespace nlsb

@@ -1,0 +1,905 @@
+// 2-D fast path: warp-level row marching. Included inside namespace nlsb.
+//
+// A warp owns a strip of columns [xs, xs + NV*W) of one slot and marches down
+// rows [r0, r1). Lane l (1 <= l <= W) owns the NV consecutive columns starting
+// at xs + NV*(l-1), loaded as one 16-byte vector; lanes 0 and W+1 load the
+// neighbouring vectors as halo. x-neighbours come from warp shuffles, the row
+// window lives in registers and the next rows are prefetched two rows ahead.
+// No shared memory and no block barriers: warps are independent tiles.
+//
+// The per-slot dot products of a pass are reduced by the last warp of the
+// slot to finish (atomic ticket), in a fixed tile order, and turned into the
+// Lanczos scalars of the pass; in the last pass that warp also evaluates f(T).
+
+template <typename E> struct V16 {
+  static constexpr int N = 16 / (int)sizeof(E);
+  E v[N];
+};
+
+template <typename E> __device__ __forceinline__ V16<E> vzero() {
+  V16<E> r;
+#pragma unroll
+  for (int q = 0; q < V16<E>::N; ++q) r.v[q] = zero<E>();
+  return r;
+}
+
+template <typename E> __device__ __forceinline__ V16<E> ld16(const E *p) {
+  V16<E> r;
+  const uint4 w = __ldg(reinterpret_cast<const uint4 *>(p));
+  memcpy(&r, &w, 16);
+  return r;
+}
+template <typename E> __device__ __forceinline__ void st16(E *p, const V16<E> &r) {
+  uint4 w;
+  memcpy(&w, &r, 16);
+  *reinterpret_cast<uint4 *>(p) = w;
+}
+
+template <typename R> __device__ __forceinline__ R shfl_up1(R v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename R> __device__ __forceinline__ Cx<R> shfl_up1(Cx<R> v) {
+  return Cx<R>{__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1)};
+}
+template <typename R> __device__ __forceinline__ R shfl_dn1(R v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+template <typename R> __device__ __forceinline__ Cx<R> shfl_dn1(Cx<R> v) {
+  return Cx<R>{__shfl_down_sync(0xffffffffu, v.x, 1), __shfl_down_sync(0xffffffffu, v.y, 1)};
+}
+
+// Geometry of one warp strip.
+struct Strip {
+  int nx, ny, pitch;
+  long long off;
+  int col0;      // first column of this lane's vector
+  bool lane_in;  // lane holds any in-domain column
+  bool out_lane; // lane writes outputs (1 <= lane <= W)
+  __device__ __forceinline__ bool row_ok(int r) const { return r >= 0 && r < ny; }
+  __device__ __forceinline__ long long addr(int r) const { return off + (long long)r * pitch + col0; }
+};
+
+template <typename E>
+__device__ __forceinline__ V16<E> load_row(const E *base, const Strip &S, int r) {
+  if (S.lane_in && S.row_ok(r)) return ld16(base + S.addr(r));
+  return vzero<E>();
+}
+
+// Masked five-point FV Laplacian (c == 1) on row `r` of the window (m, o, p)
+// with x-neighbours lft / rgt of the vector; differences formed first.
+template <typename E, typename R>
+__device__ __forceinline__ void lap_row(const Strip &S, int r, const V16<E> &m, const V16<E> &o,
+                                        const V16<E> &p, E lft, E rgt, R scl, V16<E> &out) {
+  constexpr int N = V16<E>::N;
+  const bool pm = r > 0, pp = r < S.ny - 1;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    const int x = S.col0 + q;
+    const E c = o.v[q];
+    E acc = zero<E>();
+    const E xl = q == 0 ? lft : o.v[q - 1];
+    const E xr = q == N - 1 ? rgt : o.v[q + 1];
+    if (x > 0) acc = add(acc, sub(xl, c));
+    if (x < S.nx - 1) acc = add(acc, sub(xr, c));
+    if (pm) acc = add(acc, sub(m.v[q], c));
+    if (pp) acc = add(acc, sub(p.v[q], c));
+    out.v[q] = scale(acc, scl);
+  }
+}
+
+// c-field rows carry the N reals matching one element vector.
+template <typename E> struct CRow {
+  using R = typename Traits<E>::R;
+  static constexpr int N = V16<E>::N;
+  R v[N];
+};
+template <typename E>
+__device__ __forceinline__ CRow<E> load_crow(const typename Traits<E>::R *base, const Strip &S, int r) {
+  using R = typename Traits<E>::R;
+  CRow<E> o;
+  if (S.lane_in && S.row_ok(r)) {
+    const R *p = base + S.addr(r);
+    if constexpr (sizeof(R) * CRow<E>::N == 16) {
+      const uint4 w = __ldg(reinterpret_cast<const uint4 *>(p));
+      memcpy(&o, &w, 16);
+    } else if constexpr (sizeof(R) * CRow<E>::N == 8) {
+      const uint2 w = __ldg(reinterpret_cast<const uint2 *>(p));
+      memcpy(&o, &w, 8);
+    } else {
+#pragma unroll
+      for (int q = 0; q < CRow<E>::N; ++q) o.v[q] = __ldg(p + q);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < CRow<E>::N; ++q) o.v[q] = R(0);
+  }
+  return o;
+}
+
+// Masked FV operator with a c field: cbar = (c_i + c_j)/2 per edge.
+template <typename E, typename R>
+__device__ __forceinline__ void lap_row_c(const Strip &S, int r, const V16<E> &m, const V16<E> &o,
+                                          const V16<E> &p, E lft, E rgt, const CRow<E> &cm,
+                                          const CRow<E> &co, const CRow<E> &cp, R cl, R cr, R scl,
+                                          V16<E> &out) {
+  constexpr int N = V16<E>::N;
+  const bool pm = r > 0, pp = r < S.ny - 1;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    const int x = S.col0 + q;
+    const E c = o.v[q];
+    const R ci = co.v[q];
+    E acc = zero<E>();
+    const E xl = q == 0 ? lft : o.v[q - 1];
+    const E xr = q == N - 1 ? rgt : o.v[q + 1];
+    const R cxl = q == 0 ? cl : co.v[q - 1];
+    const R cxr = q == N - 1 ? cr : co.v[q + 1];
+    if (x > 0) acc = fma_s((cxl + ci) * R(0.5), sub(xl, c), acc);
+    if (x < S.nx - 1) acc = fma_s((cxr + ci) * R(0.5), sub(xr, c), acc);
+    if (pm) acc = fma_s((cm.v[q] + ci) * R(0.5), sub(m.v[q], c), acc);
+    if (pp) acc = fma_s((cp.v[q] + ci) * R(0.5), sub(p.v[q], c), acc);
+    out.v[q] = scale(acc, scl);
+  }
+}
+
+// Operator on row r of the window (m, o, p); cw: c rows r-1, r, r+1.
+template <typename E, typename R, bool HC>
+__device__ __forceinline__ void lap_any(const Strip &S, int r, const V16<E> &m, const V16<E> &o,
+                                        const V16<E> &p, const CRow<E> *cw, R scl, V16<E> &out) {
+  constexpr int N = V16<E>::N;
+  const E lft = shfl_up1(o.v[N - 1]);
+  const E rgt = shfl_dn1(o.v[0]);
+  if constexpr (!HC) {
+    lap_row<E, R>(S, r, m, o, p, lft, rgt, scl, out);
+  } else {
+    const R cl = shfl_up1(cw[1].v[N - 1]);
+    const R cr = shfl_dn1(cw[1].v[0]);
+    lap_row_c<E, R>(S, r, m, o, p, lft, rgt, cw[0], cw[1], cw[2], cl, cr, scl, out);
+  }
+}
+
+// Warp-level tile of a slot.
+// TileDesc of a 2-D warp strip: x0 = first column xs, y0 = output lanes W,
+// [p0, p1) = rows.
+template <int N>
+__device__ __forceinline__ Strip make_strip(const SlotDesc &s, const TileDesc &t, int lane) {
+  Strip S;
+  S.nx = s.nx;
+  S.ny = s.ny;
+  S.pitch = s.pitch;
+  S.off = s.off;
+  S.col0 = t.x0 + N * (lane - 1);
+  S.lane_in = lane <= t.y0 + 1 && S.col0 + N > 0 && S.col0 < s.nx;
+  S.out_lane = lane >= 1 && lane <= t.y0 && S.col0 < s.nx;
+  return S;
+}
+
+// --------------------------------------------------- last-warp slot reduce
+// Every warp writes its NVAL partial sums; the warp that takes the last ticket
+// of the slot sums all of them in tile order, so the result does not depend on
+// which warp finishes last.
+template <int NVAL>
+__device__ __forceinline__ bool warp_publish(double *vals, double *part, int tile, int *ticket,
+                                             int tile_count, int lane) {
+#pragma unroll
+  for (int q = 0; q < NVAL; ++q) {
+    double v = vals[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    vals[q] = v;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NVAL; ++q) __stcg(part + (long long)tile * NVAL + q, vals[q]);
+  }
+  __threadfence();
+  int last = 0;
+  if (lane == 0) last = atomicAdd(ticket, 1) == tile_count - 1;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (last) __threadfence();
+  return last != 0;
+}
+
+// Sum the partials of tiles [tb, tb+tc) in tile order: lane q < NVAL owns value q.
+template <int NVAL>
+__device__ __forceinline__ double warp_slot_total(const double *part, int tb, int tc, int lane) {
+  double s = 0.0;
+  if (lane < NVAL) {
+    int t = 0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    // four independent chains keep the L2 loads in flight; combined in a fixed order
+    for (; t + 4 <= tc; t += 4) {
+      a0 += __ldcg(part + (long long)(tb + t) * NVAL + lane);
+      a1 += __ldcg(part + (long long)(tb + t + 1) * NVAL + lane);
+      a2 += __ldcg(part + (long long)(tb + t + 2) * NVAL + lane);
+      a3 += __ldcg(part + (long long)(tb + t + 3) * NVAL + lane);
+    }
+    for (; t < tc; ++t) a0 += __ldcg(part + (long long)(tb + t) * NVAL + lane);
+    s = (a0 + a1) + (a2 + a3);
+  }
+  return s;
+}
+
+constexpr int WPB = 4;  // warps per block of the 2-D kernels
+
+template <typename E> __device__ __forceinline__ V16<E> vscale(const V16<E> &a, typename Traits<E>::R s) {
+  V16<E> r;
+#pragma unroll
+  for (int q = 0; q < V16<E>::N; ++q) r.v[q] = scale(a.v[q], s);
+  return r;
+}
+
+// Mask elements outside the domain (columns >= nx or < 0, or rows outside).
+template <typename E> __device__ __forceinline__ void vmask(V16<E> &a, const Strip &S, int r) {
+  const bool rok = S.row_ok(r);
+#pragma unroll
+  for (int q = 0; q < V16<E>::N; ++q) {
+    const int x = S.col0 + q;
+    if (!(rok && x >= 0 && x < S.nx)) a.v[q] = zero<E>();
+  }
+}
+
+// Per-row dot accumulation: partial sums over the N elements in R, then one
+// Kahan update per row. Layout as NDot (real 6 / complex 9 per sequence).
+template <typename R>
+__device__ __forceinline__ void dots_row(Kahan<R> *k, const V16<R> &z, const V16<R> &vj, const V16<R> &vm) {
+  R s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+#pragma unroll
+  for (int q = 0; q < V16<R>::N; ++q) {
+    s0 = fma(z.v[q], vm.v[q], s0);
+    s1 = fma(z.v[q], vj.v[q], s1);
+    s2 = fma(vm.v[q], vj.v[q], s2);
+    s3 = fma(z.v[q], z.v[q], s3);
+    s4 = fma(vj.v[q], vj.v[q], s4);
+    s5 = fma(vm.v[q], vm.v[q], s5);
+  }
+  k[0].add(s0); k[1].add(s1); k[2].add(s2); k[3].add(s3); k[4].add(s4); k[5].add(s5);
+}
+template <typename R>
+__device__ __forceinline__ void dots_row(Kahan<R> *k, const V16<Cx<R>> &z, const V16<Cx<R>> &vj,
+                                         const V16<Cx<R>> &vm) {
+  R s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int q = 0; q < V16<Cx<R>>::N; ++q) {
+    const Cx<R> a = z.v[q], b = vj.v[q], c = vm.v[q];
+    s[0] += a.x * c.x + a.y * c.y;  // conj(z) v_{j-1}
+    s[1] += a.x * c.y - a.y * c.x;
+    s[2] += a.x * b.x + a.y * b.y;  // conj(z) v_j
+    s[3] += a.x * b.y - a.y * b.x;
+    s[4] += c.x * b.x + c.y * b.y;  // conj(v_{j-1}) v_j
+    s[5] += c.x * b.y - c.y * b.x;
+    s[6] += a.x * a.x + a.y * a.y;
+    s[7] += b.x * b.x + b.y * b.y;
+    s[8] += c.x * c.x + c.y * c.y;
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) k[q].add(s[q]);
+}
+
+// Finish a pass in the last warp of the slot: totals -> Lanczos scalars of
+// pass j (table entry j), beta0 for the first pass; reset the ticket.
+template <typename E, int NSEQ>
+__device__ __forceinline__ void finish_pass(const StepArgs &a, int slot, int j, const SlotDesc &s,
+                                            int lane) {
+  using R = typename Traits<E>::R;
+  constexpr bool CP = Traits<E>::cplx;
+  constexpr int ND = NDot<E>::value, NV = ND * NSEQ;
+  const double *part = a.part + (long long)j * a.part_stride;
+  const double tot = warp_slot_total<NV>(part, s.tile_begin, s.tile_count, lane);
+  double tv[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+  if (lane < NSEQ) {
+    const int sq = lane;
+    LzScal L;
+    if (j == 0) {
+      double b0;
+      L = lz_first<CP>(tv + sq * ND, Eps<R>::v, b0);
+      a.beta0[slot * 2 + sq] = b0;
+    } else {
+      L = lz_from_dots<CP>(tv + sq * ND, Eps<R>::v);
+    }
+    a.scal[(slot * 2 + sq) * KMAX + j] = L;
+  }
+  if (lane == 0) a.ticket[slot] = 0;
+}
+
+// Source rows of the first pass (the vectors to which f(A) is applied): the
+// raw field rows are loaded ahead (load) and turned into sources later (make).
+template <int SRC, typename E> struct SrcRow;
+
+template <typename R> struct SrcRow<SRC_KG, R> {
+  // seq 0: u; seq 1: g(u) = (p1 m + q1) u + (p3 m + q3) u^3 + (rm m + r0) xi
+  static constexpr int NSEQ = 2;
+  struct Raw {
+    V16<R> u;
+    CRow<R> m;
+  };
+  static __device__ __forceinline__ Raw load(const StepArgs &a, const Strip &S, int r) {
+    return Raw{load_row((const R *)a.f.u_hi, S, r), load_crow<R>((const R *)a.f.m, S, r)};
+  }
+  static __device__ __forceinline__ void make(const Raw &w, const SlotDesc &s, const Strip &S,
+                                              int step, int r, V16<R> *x) {
+    constexpr int N = V16<R>::N;
+    const bool noisy = s.rm != 0.0 || s.r0 != 0.0;
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const R u = w.u.v[q], mm = w.m.v[q];
+      R g = (R(s.p1) * mm + R(s.q1)) * u + (R(s.p3) * mm + R(s.q3)) * (u * u * u);
+      if (noisy) {
+        const int xx = S.col0 + q;
+        if (S.row_ok(r) && xx >= 0 && xx < S.nx)
+          g += (R(s.rm) * mm + R(s.r0)) *
+               philox_normal<R>(s.seed, (uint32_t)step, (uint32_t)((long long)r * S.nx + xx));
+      }
+      x[0].v[q] = u;
+      x[1].v[q] = g;
+    }
+    vmask(x[0], S, r);
+    vmask(x[1], S, r);
+  }
+};
+template <typename R> struct SrcRow<SRC_SS2, Cx<R>> {
+  // N_{tau/2}(u) = u exp(i tau/2 rho), rho = (p3 m + q3)|u|^2 (nlse_dev.hpp:20-41)
+  static constexpr int NSEQ = 1;
+  struct Raw {
+    V16<Cx<R>> u;
+    CRow<Cx<R>> m;
+  };
+  static __device__ __forceinline__ Raw load(const StepArgs &a, const Strip &S, int r) {
+    return Raw{load_row((const Cx<R> *)a.f.u_hi, S, r), load_crow<Cx<R>>((const R *)a.f.m, S, r)};
+  }
+  static __device__ __forceinline__ void make(const Raw &w, const SlotDesc &s, const Strip &S, int,
+                                              int r, V16<Cx<R>> *x) {
+#pragma unroll
+    for (int q = 0; q < V16<Cx<R>>::N; ++q) {
+      const Cx<R> u = w.u.v[q];
+      const R phi = R(0.5 * s.dt) * ((R(s.p3) * w.m.v[q] + R(s.q3)) * norm2(u));
+      const R sn = sin(phi), cs = cos(phi);
+      x[0].v[q] = Cx<R>{u.x * cs - u.y * sn, u.x * sn + u.y * cs};
+    }
+    vmask(x[0], S, r);
+  }
+};
+template <typename R> struct SrcRow<SRC_SEWI_A, Cx<R>> {
+  // seq 0: B(u) = -rho u (nlse_dev.hpp:43-52); seq 1: u_prev
+  static constexpr int NSEQ = 2;
+  struct Raw {
+    V16<Cx<R>> u, up;
+    CRow<Cx<R>> m;
+  };
+  static __device__ __forceinline__ Raw load(const StepArgs &a, const Strip &S, int r) {
+    return Raw{load_row((const Cx<R> *)a.f.u_hi, S, r), load_row((const Cx<R> *)a.f.up_hi, S, r),
+               load_crow<Cx<R>>((const R *)a.f.m, S, r)};
+  }
+  static __device__ __forceinline__ void make(const Raw &w, const SlotDesc &s, const Strip &S, int,
+                                              int r, V16<Cx<R>> *x) {
+#pragma unroll
+    for (int q = 0; q < V16<Cx<R>>::N; ++q) {
+      const R rr = -((R(s.p3) * w.m.v[q] + R(s.q3)) * norm2(w.u.v[q]));
+      x[0].v[q] = Cx<R>{rr * w.u.v[q].x, rr * w.u.v[q].y};
+    }
+    x[1] = w.up;
+    vmask(x[0], S, r);
+    vmask(x[1], S, r);
+  }
+};
+template <typename R> struct SrcRow<SRC_SEWI_B, Cx<R>> {
+  static constexpr int NSEQ = 1;
+  struct Raw {
+    V16<Cx<R>> y;
+  };
+  static __device__ __forceinline__ Raw load(const StepArgs &a, const Strip &S, int r) {
+    return Raw{load_row((const Cx<R> *)a.f.ya, S, r)};
+  }
+  static __device__ __forceinline__ void make(const Raw &w, const SlotDesc &, const Strip &S, int,
+                                              int r, V16<Cx<R>> *x) {
+    x[0] = w.y;
+    vmask(x[0], S, r);
+  }
+};
+
+#define WARP_TILE_PROLOGUE                                                           \
+  const int lane = threadIdx.x & 31;                                                 \
+  const int wt = blockIdx.x * WPB + (threadIdx.x >> 5);                              \
+  if (wt >= *a.ntiles) return;                                                       \
+  const TileDesc t = a.tiles[wt];                                                    \
+  const SlotDesc &s = a.slots[t.slot];                                               \
+  const Strip S = make_strip<V16<E>::N>(s, t, lane);                                 \
+  const int step = a.state[t.slot].step;                                             \
+  (void)step;
+
+// ---------------------------------------------------------------- first pass
+// x = source rows, V_0 = x, z = A x, dots <A x, x>, |A x|^2, |x|^2 per sequence.
+template <typename E, int SRC, bool HC>
+__global__ void __launch_bounds__(32 * WPB) k2_first(StepArgs a) {
+  using R = typename Traits<E>::R;
+  using SR = SrcRow<SRC, E>;
+  constexpr int NSEQ = SR::NSEQ;
+  constexpr int ND = NDot<E>::value, NV = ND * NSEQ;
+  WARP_TILE_PROLOGUE
+  const R opsc = R(a.op_sign * s.inv_h2);
+  const R *cf = (const R *)a.f.c;
+  V16<E> xm[NSEQ], xo[NSEQ], xp[NSEQ];
+  CRow<E> cw[3], cn1, cn2;
+  Kahan<R> acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) acc[q].init();
+  const int r0 = t.p0, r1 = t.p1;
+  typename SR::Raw w1 = SR::load(a, S, r0 + 1), w2 = SR::load(a, S, r0 + 2);
+  SR::make(SR::load(a, S, r0 - 1), s, S, step, r0 - 1, xo);
+  SR::make(SR::load(a, S, r0), s, S, step, r0, xp);
+  if constexpr (HC) {
+    cw[1] = load_crow<E>(cf, S, r0 - 1);
+    cw[2] = load_crow<E>(cf, S, r0);
+    cn1 = load_crow<E>(cf, S, r0 + 1);
+    cn2 = load_crow<E>(cf, S, r0 + 2);
+  }
+  for (int r = r0; r < r1; ++r) {
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      xm[sq] = xo[sq];
+      xo[sq] = xp[sq];
+    }
+    SR::make(w1, s, S, step, r + 1, xp);
+    w1 = w2;
+    w2 = SR::load(a, S, r + 3);
+    if constexpr (HC) {
+      cw[0] = cw[1];
+      cw[1] = cw[2];
+      cw[2] = cn1;
+      cn1 = cn2;
+      cn2 = load_crow<E>(cf, S, r + 3);
+    }
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      V16<E> z;
+      lap_any<E, R, HC>(S, r, xm[sq], xo[sq], xp[sq], cw, opsc, z);
+      vmask(z, S, r);
+      if (S.out_lane) {
+        st16((E *)a.V + (long long)(sq * a.kv) * a.vstride + S.addr(r), xo[sq]);
+        dots_row(acc + sq * ND, z, xo[sq], vzero<E>());
+      }
+    }
+  }
+  double vals[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) vals[q] = S.out_lane ? acc[q].val() : 0.0;
+  if (warp_publish<NV>(vals, a.part, wt, a.ticket + t.slot, s.tile_count, lane))
+    finish_pass<E, NSEQ>(a, t.slot, 0, s, lane);
+}
+
+// ------------------------------------------------------- Lanczos pass j >= 1
+// v_j(q) = (sA A V_{j-1}(q) - a sA V_{j-1}(q) - d sB V_{j-2}(q)) inv_b on rows
+// q = r0-1 .. r1 (V_{j-1} rows r0-2 .. r1+1), z_j = A v_j on rows r0 .. r1-1.
+template <typename E, int NSEQ, bool HC>
+__global__ void __launch_bounds__(32 * WPB) k2_lanczos(StepArgs a) {
+  using R = typename Traits<E>::R;
+  constexpr int ND = NDot<E>::value, NV = ND * NSEQ;
+  WARP_TILE_PROLOGUE
+  const int j = a.j;
+  const R opsc = R(a.op_sign * s.inv_h2);
+  const R *cf = (const R *)a.f.c;
+  // scalars of pass j-1 (published by its last warp)
+  R sA[NSEQ], sB[NSEQ], ar[NSEQ], ai[NSEQ], dr[NSEQ], di[NSEQ], ib[NSEQ];
+  const E *VA[NSEQ];
+  const E *VB[NSEQ];
+  E *VJ[NSEQ];
+#pragma unroll
+  for (int sq = 0; sq < NSEQ; ++sq) {
+    const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+    const double b0 = a.beta0[t.slot * 2 + sq];
+    const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+    sA[sq] = R(j == 1 ? s0 : 1.0);
+    sB[sq] = R(j == 2 ? s0 : 1.0);
+    ar[sq] = R(L.ar);
+    ai[sq] = R(L.ai);
+    dr[sq] = R(L.dr);
+    di[sq] = R(L.di);
+    ib[sq] = R(L.inv_b);
+    VA[sq] = (const E *)a.V + (long long)(sq * a.kv + j - 1) * a.vstride;
+    VB[sq] = (const E *)a.V + (long long)(sq * a.kv + (j >= 2 ? j - 2 : 0)) * a.vstride;
+    VJ[sq] = (E *)a.V + (long long)(sq * a.kv + j) * a.vstride;
+  }
+  // windows: A rows q-1, q, q+1 (+ two prefetched), B row q (+ two prefetched),
+  // v_j rows r-1, r, r+1 where q = r + 1
+  V16<E> A0[NSEQ], A1[NSEQ], A2[NSEQ], An1[NSEQ], An2[NSEQ];
+  V16<E> B0[NSEQ], Bn1[NSEQ], Bn2[NSEQ];
+  V16<E> Vm[NSEQ], Vo[NSEQ], Vp[NSEQ];
+  CRow<E> cA[3], cn1, cn2, cV[3];
+  Kahan<R> acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) acc[q].init();
+  const int r0 = t.p0, r1 = t.p1;
+#pragma unroll
+  for (int sq = 0; sq < NSEQ; ++sq) {
+    A0[sq] = load_row(VA[sq], S, r0 - 2);
+    A1[sq] = load_row(VA[sq], S, r0 - 1);
+    A2[sq] = load_row(VA[sq], S, r0);
+    An1[sq] = load_row(VA[sq], S, r0 + 1);
+    An2[sq] = load_row(VA[sq], S, r0 + 2);
+    if (j >= 2) {
+      B0[sq] = load_row(VB[sq], S, r0 - 1);
+      Bn1[sq] = load_row(VB[sq], S, r0);
+      Bn2[sq] = load_row(VB[sq], S, r0 + 1);
+    } else {
+      B0[sq] = Bn1[sq] = Bn2[sq] = vzero<E>();
+    }
+    Vo[sq] = vzero<E>();
+    Vp[sq] = vzero<E>();
+  }
+  if constexpr (HC) {
+    cA[0] = load_crow<E>(cf, S, r0 - 2);
+    cA[1] = load_crow<E>(cf, S, r0 - 1);
+    cA[2] = load_crow<E>(cf, S, r0);
+    cn1 = load_crow<E>(cf, S, r0 + 1);
+    cn2 = load_crow<E>(cf, S, r0 + 2);
+    // cV is fully rotated in before its first use (three shifts)
+    cV[0] = cV[1] = cV[2] = cA[0];
+  }
+  for (int r = r0 - 2; r < r1; ++r) {
+    const int q = r + 1;
+    // (a) v_j on row q
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      V16<E> w;
+      lap_any<E, R, HC>(S, q, A0[sq], A1[sq], A2[sq], cA, opsc, w);
+      V16<E> v;
+#pragma unroll
+      for (int e = 0; e < V16<E>::N; ++e) {
+        E x = scale(w.v[e], sA[sq]);
+        x = cfma(-ar[sq], -ai[sq], scale(A1[sq].v[e], sA[sq]), x);
+        x = cfma(-dr[sq], -di[sq], scale(B0[sq].v[e], sB[sq]), x);
+        v.v[e] = scale(x, ib[sq]);
+      }
+      vmask(v, S, q);
+      Vm[sq] = Vo[sq];
+      Vo[sq] = Vp[sq];
+      Vp[sq] = v;
+      if (S.out_lane && q >= r0 && q < r1) st16(VJ[sq] + S.addr(q), v);
+    }
+    if constexpr (HC) {
+      cV[0] = cV[1];
+      cV[1] = cV[2];
+      cV[2] = cA[1];
+    }
+    // (b) z_j = A v_j on row r and the dots (v_{j-1}(r) = sA A0 before the shift)
+    if (r >= r0) {
+#pragma unroll
+      for (int sq = 0; sq < NSEQ; ++sq) {
+        V16<E> z;
+        lap_any<E, R, HC>(S, r, Vm[sq], Vo[sq], Vp[sq], cV, opsc, z);
+        vmask(z, S, r);
+        if (S.out_lane) dots_row(acc + sq * ND, z, Vo[sq], vscale(A0[sq], sA[sq]));
+      }
+    }
+    // (c) shift the A / B windows and prefetch two rows ahead
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      A0[sq] = A1[sq];
+      A1[sq] = A2[sq];
+      A2[sq] = An1[sq];
+      An1[sq] = An2[sq];
+      An2[sq] = load_row(VA[sq], S, q + 4);
+      B0[sq] = Bn1[sq];
+      Bn1[sq] = Bn2[sq];
+      Bn2[sq] = j >= 2 ? load_row(VB[sq], S, q + 3) : vzero<E>();
+    }
+    if constexpr (HC) {
+      cA[0] = cA[1];
+      cA[1] = cA[2];
+      cA[2] = cn1;
+      cn1 = cn2;
+      cn2 = load_crow<E>(cf, S, q + 4);
+    }
+  }
+  double vals[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) vals[q] = S.out_lane ? acc[q].val() : 0.0;
+  if (warp_publish<NV>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot,
+                       s.tile_count, lane))
+    finish_pass<E, NSEQ>(a, t.slot, j, s, lane);
+}
+
+// ------------------------------------------------------------ final pass
+template <typename R> __device__ __forceinline__ R coef_w(const FinalCoef &F, int q, bool im);
+template <> __device__ __forceinline__ float coef_w<float>(const FinalCoef &F, int q, bool im) {
+  return im ? F.wi32[q] : F.wr32[q];
+}
+template <> __device__ __forceinline__ double coef_w<double>(const FinalCoef &F, int q, bool im) {
+  return im ? F.wi[q] : F.wr[q];
+}
+
+template <int FIN, typename E> struct FinRow;
+
+template <typename R> struct FinRow<FIN_KG, R> {
+  // Gautschi (kg_single.cuh:101-126) with d = u - u_past:
+  // d+ = d + 2 (cos(tau sqrt A) - I) u + tau^2 sinc^2(tau sqrt A) g(u), u+ = u + d+.
+  static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
+                                               int step, int r, const V16<R> *y) {
+    constexpr int N = V16<R>::N;
+    R *uh = (R *)a.f.u_hi + S.addr(r), *ul = (R *)a.f.u_lo + S.addr(r), *dd = (R *)a.f.d + S.addr(r);
+    V16<R> hi = ld16((const R *)uh), lo = ld16((const R *)ul), d = ld16((const R *)dd);
+    const R dt = R(s.dt), t2 = dt * dt;
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const R dp = d.v[q] + R(2) * y[0].v[q] + t2 * y[1].v[q];
+      comp_add(hi.v[q], lo.v[q], dp);
+      d.v[q] = dp;
+    }
+    vmask(d, S, r);
+    st16(uh, hi);
+    st16(ul, lo);
+    st16(dd, d);
+    int fr;
+    if (snap_step(s, step, fr)) {
+      double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const int x = S.col0 + q;
+        if (x >= 0 && x < S.nx) {
+          const long long pt = (long long)r * S.nx + x;
+          SN[pt] = (double)hi.v[q] + (double)lo.v[q];
+          SN[s.n + pt] = (double)d.v[q] / s.dt;
+        }
+      }
+    }
+  }
+};
+
+template <typename R> struct FinRow<FIN_SS2, Cx<R>> {
+  // u <- N_{tau/2}(e^{i tau L} N_{tau/2}(u)) accumulated as u += D1 + I + D2
+  // (nlse_dev.hpp:187-203), D1 = u(e^{i phi1}-1), D2 = w(e^{i phi2}-1), w = N(u)+I.
+  static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
+                                               int step, int r, const V16<Cx<R>> *y) {
+    constexpr int N = V16<Cx<R>>::N;
+    Cx<R> *uh = (Cx<R> *)a.f.u_hi + S.addr(r), *ul = (Cx<R> *)a.f.u_lo + S.addr(r);
+    V16<Cx<R>> hi = ld16((const Cx<R> *)uh), lo = ld16((const Cx<R> *)ul);
+    const CRow<Cx<R>> m = load_crow<Cx<R>>((const R *)a.f.m, S, r);
+    const R half = R(0.5 * s.dt);
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const R kap = R(s.p3) * m.v[q] + R(s.q3);
+      const Cx<R> d1 = cexpm1_mul(hi.v[q], half * (kap * norm2(hi.v[q])));
+      const Cx<R> w = add(add(hi.v[q], d1), y[0].v[q]);
+      const Cx<R> d2 = cexpm1_mul(w, half * (kap * norm2(w)));
+      comp_add(hi.v[q], lo.v[q], add(add(d1, y[0].v[q]), d2));
+    }
+    vmask(hi, S, r);
+    vmask(lo, S, r);
+    st16(uh, hi);
+    st16(ul, lo);
+    int fr;
+    if (snap_step(s, step, fr)) {
+      double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const int x = S.col0 + q;
+        if (x >= 0 && x < S.nx) {
+          const long long pt = (long long)r * S.nx + x;
+          SN[2 * pt] = (double)hi.v[q].x + (double)lo.v[q].x;
+          SN[2 * pt + 1] = (double)hi.v[q].y + (double)lo.v[q].y;
+        }
+      }
+    }
+  }
+};
+
+template <typename R> struct FinRow<FIN_SEWI_A, Cx<R>> {
+  // y_a = sinc(tau L) B(u), I2 = (e^{2 i tau L} - I) u_prev (nlse_dev.hpp:215-223)
+  static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &, const Strip &S, int,
+                                               int r, const V16<Cx<R>> *y) {
+    st16((Cx<R> *)a.f.ya + S.addr(r), y[0]);
+    st16((Cx<R> *)a.f.ib + S.addr(r), y[1]);
+  }
+};
+
+template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
+  // y_b = e^{i tau L} y_a, y_2 = u_prev + I2; u+ = y_b - 2 i tau y_2 (reference
+  // operand order, nlse_dev.hpp:54-64 called at :225) or y_2 - 2 i tau y_b.
+  static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
+                                               int step, int r, const V16<Cx<R>> *y) {
+    constexpr int N = V16<Cx<R>>::N;
+    const long long o = S.addr(r);
+    Cx<R> *uh = (Cx<R> *)a.f.u_hi + o, *ul = (Cx<R> *)a.f.u_lo + o;
+    Cx<R> *ph = (Cx<R> *)a.f.up_hi + o, *pl = (Cx<R> *)a.f.up_lo + o;
+    const V16<Cx<R>> i2 = ld16((const Cx<R> *)a.f.ib + o);
+    const V16<Cx<R>> uh0 = ld16((const Cx<R> *)uh), ul0 = ld16((const Cx<R> *)ul);
+    V16<Cx<R>> nh = ld16((const Cx<R> *)ph), nl = ld16((const Cx<R> *)pl);
+    const R tt = R(2.0 * s.dt);
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const Cx<R> yb = y[0].v[q];
+      if (s.variant == 0) {
+        const Cx<R> y2 = add(nh.v[q], i2.v[q]);
+        const Cx<R> h = Cx<R>{yb.x + tt * y2.y, yb.y - tt * y2.x};
+        const Cx<R> l = Cx<R>{tt * nl.v[q].y, -tt * nl.v[q].x};
+        R sx, ex, sy, ey;
+        two_sum(h.x, l.x, sx, ex);
+        two_sum(h.y, l.y, sy, ey);
+        nh.v[q] = Cx<R>{sx, sy};
+        nl.v[q] = Cx<R>{ex, ey};
+      } else {
+        comp_add(nh.v[q], nl.v[q], Cx<R>{i2.v[q].x + tt * yb.y, i2.v[q].y - tt * yb.x});
+      }
+    }
+    vmask(nh, S, r);
+    vmask(nl, S, r);
+    st16(ph, uh0);
+    st16(pl, ul0);
+    st16(uh, nh);
+    st16(ul, nl);
+    int fr;
+    if (snap_step(s, step, fr)) {
+      double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const int x = S.col0 + q;
+        if (x >= 0 && x < S.nx) {
+          const long long pt = (long long)r * S.nx + x;
+          SN[2 * pt] = (double)nh.v[q].x + (double)nl.v[q].x;
+          SN[2 * pt + 1] = (double)nh.v[q].y + (double)nl.v[q].y;
+        }
+      }
+    }
+  }
+};
+
+// y_seq = sum_{q < kv-1} W_q V_q + W_{kv-1} V_{kv-1} + Lam (A V_{kv-1}); V_{kv-1}
+// is marched with a one-row window, the other vectors are read at the row only.
+template <typename E, int NSEQ, int FIN, bool HC>
+__global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
+  using R = typename Traits<E>::R;
+  WARP_TILE_PROLOGUE
+  const int kv = a.kv;
+  const R opsc = R(a.op_sign * s.inv_h2);
+  const R *cf = (const R *)a.f.c;
+  const FinalCoef *FC[NSEQ];
+  const E *VL[NSEQ];
+  R lr[NSEQ], li[NSEQ], wlr[NSEQ], wli[NSEQ];
+#pragma unroll
+  for (int sq = 0; sq < NSEQ; ++sq) {
+    FC[sq] = a.coef + t.slot * 2 + sq;
+    VL[sq] = (const E *)a.V + (long long)(sq * kv + kv - 1) * a.vstride;
+    if constexpr (sizeof(R) == 4) {
+      lr[sq] = FC[sq]->lam32[0];
+      li[sq] = FC[sq]->lam32[1];
+    } else {
+      lr[sq] = R(FC[sq]->lam_r);
+      li[sq] = R(FC[sq]->lam_i);
+    }
+    wlr[sq] = coef_w<R>(*FC[sq], kv - 1, false);
+    wli[sq] = coef_w<R>(*FC[sq], kv - 1, true);
+  }
+  V16<E> Lm[NSEQ], Lo[NSEQ], Lp[NSEQ], Ln1[NSEQ], Ln2[NSEQ];
+  CRow<E> cw[3], cn1, cn2;
+  const int r0 = t.p0, r1 = t.p1;
+#pragma unroll
+  for (int sq = 0; sq < NSEQ; ++sq) {
+    Lo[sq] = load_row(VL[sq], S, r0 - 1);
+    Lp[sq] = load_row(VL[sq], S, r0);
+    Ln1[sq] = load_row(VL[sq], S, r0 + 1);
+    Ln2[sq] = load_row(VL[sq], S, r0 + 2);
+  }
+  if constexpr (HC) {
+    cw[1] = load_crow<E>(cf, S, r0 - 1);
+    cw[2] = load_crow<E>(cf, S, r0);
+    cn1 = load_crow<E>(cf, S, r0 + 1);
+    cn2 = load_crow<E>(cf, S, r0 + 2);
+  }
+  for (int r = r0; r < r1; ++r) {
+    V16<E> y[NSEQ];
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      Lm[sq] = Lo[sq];
+      Lo[sq] = Lp[sq];
+      Lp[sq] = Ln1[sq];
+      Ln1[sq] = Ln2[sq];
+      Ln2[sq] = load_row(VL[sq], S, r + 3);
+    }
+    if constexpr (HC) {
+      cw[0] = cw[1];
+      cw[1] = cw[2];
+      cw[2] = cn1;
+      cn1 = cn2;
+      cn2 = load_crow<E>(cf, S, r + 3);
+    }
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      V16<E> z;
+      lap_any<E, R, HC>(S, r, Lm[sq], Lo[sq], Lp[sq], cw, opsc, z);
+      V16<E> acc;
+#pragma unroll
+      for (int e = 0; e < V16<E>::N; ++e)
+        acc.v[e] = cfma(wlr[sq], wli[sq], Lo[sq].v[e], cmul(lr[sq], li[sq], z.v[e]));
+      if (S.lane_in) {
+        const E *Vb = (const E *)a.V + (long long)(sq * kv) * a.vstride + S.addr(r);
+        for (int q = 0; q < kv - 1; ++q) {
+          const V16<E> vq = ld16(Vb + (long long)q * a.vstride);
+          const R wr = coef_w<R>(*FC[sq], q, false), wi = coef_w<R>(*FC[sq], q, true);
+#pragma unroll
+          for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vq.v[e], acc.v[e]);
+        }
+      }
+      vmask(acc, S, r);
+      y[sq] = acc;
+    }
+    if (S.out_lane && S.row_ok(r)) FinRow<FIN, E>::apply(a, s, S, step, r, y);
+  }
+}
+
+// ------------------------------------------------------- Stormer-Verlet
+// kg_single.cuh:145-178 / stochastic_phi4.cuh:19-77 in increment form:
+// d+ = d + tau^2 (L u + g(u)), u+ = u + d+, v = d+/tau. The hi part of u
+// alternates between two buffers by step parity so that no warp overwrites a
+// row another warp still reads as halo.
+template <typename R, bool HC>
+__global__ void __launch_bounds__(32 * WPB) k2_sv(StepArgs a) {
+  using E = R;
+  constexpr int N = V16<R>::N;
+  WARP_TILE_PROLOGUE
+  const R *U = (const R *)((step & 1) ? a.f.u_hi : a.f.u_alt);
+  R *Unew = (R *)((step & 1) ? a.f.u_alt : a.f.u_hi);
+  const R *cf = (const R *)a.f.c;
+  const R scl = R(s.inv_h2);
+  const R dt = R(s.dt), t2 = dt * dt;
+  const bool noisy = s.rm != 0.0 || s.r0 != 0.0;
+  V16<R> Um, Uo, Up, Un1, Un2;
+  CRow<R> cw[3], cn1, cn2;
+  const int r0 = t.p0, r1 = t.p1;
+  Uo = load_row(U, S, r0 - 1);
+  Up = load_row(U, S, r0);
+  Un1 = load_row(U, S, r0 + 1);
+  Un2 = load_row(U, S, r0 + 2);
+  if constexpr (HC) {
+    cw[1] = load_crow<R>(cf, S, r0 - 1);
+    cw[2] = load_crow<R>(cf, S, r0);
+    cn1 = load_crow<R>(cf, S, r0 + 1);
+    cn2 = load_crow<R>(cf, S, r0 + 2);
+  }
+  for (int r = r0; r < r1; ++r) {
+    Um = Uo;
+    Uo = Up;
+    Up = Un1;
+    Un1 = Un2;
+    Un2 = load_row(U, S, r + 3);
+    if constexpr (HC) {
+      cw[0] = cw[1];
+      cw[1] = cw[2];
+      cw[2] = cn1;
+      cn1 = cn2;
+      cn2 = load_crow<R>(cf, S, r + 3);
+    }
+    V16<R> lu;
+    lap_any<R, R, HC>(S, r, Um, Uo, Up, cw, scl, lu);
+    if (!(S.out_lane && S.row_ok(r))) continue;
+    const long long o = S.addr(r);
+    V16<R> lo = ld16((const R *)a.f.u_lo + o), d = ld16((const R *)a.f.d + o), hi = Uo;
+    const CRow<R> m = load_crow<R>((const R *)a.f.m, S, r);
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      const R u = Uo.v[q], mm = m.v[q];
+      R g = (R(s.p1) * mm + R(s.q1)) * u + (R(s.p3) * mm + R(s.q3)) * (u * u * u);
+      const int x = S.col0 + q;
+      if (noisy && x >= 0 && x < S.nx)
+        g += (R(s.rm) * mm + R(s.r0)) *
+             philox_normal<R>(s.seed, (uint32_t)step, (uint32_t)((long long)r * S.nx + x));
+      const R dp = d.v[q] + t2 * (lu.v[q] + g);
+      comp_add(hi.v[q], lo.v[q], dp);
+      d.v[q] = dp;
+    }
+    vmask(d, S, r);
+    st16(Unew + o, hi);
+    st16((R *)a.f.u_lo + o, lo);
+    st16((R *)a.f.d + o, d);
+    int fr;
+    if (snap_step(s, step, fr)) {
+      double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const int x = S.col0 + q;
+        if (x >= 0 && x < S.nx) {
+          const long long pt = (long long)r * S.nx + x;
+          SN[pt] = (double)hi.v[q] + (double)lo.v[q];
+          SN[s.n + pt] = (double)d.v[q] / s.dt;
+        }
+      }
+    }
+  }
+}
