@@ -138,6 +138,11 @@ int nls_pool_step_timed(nls_pool *pool, int32_t nsteps, float *ms);
 int nls_pool_kernels_per_step(nls_pool *pool, int32_t *count);
 int nls_pool_destroy(nls_pool *pool);
 
+/* Page-locked host memory for inputs and snapshot buffers (makes admission
+   and snapshot copies asynchronous DMA). */
+int nls_host_alloc(int64_t bytes, void **out);
+int nls_host_free(void *ptr);
+
 /* Select the CUDA device for the calling thread's subsequent pools/handles
    (one process per GPU; the library keeps its own runtime state). */
 int nls_set_device(int32_t device);

@@ -90,6 +90,11 @@ cudaError_t launch2_lanczos(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_lanczos<E, NSEQ, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
+template <typename E, bool HC>
+cudaError_t launch2_lanczos1(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_lanczos1<E, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
 template <typename E, int NSEQ, int FIN, bool HC>
 cudaError_t launch2_final(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_final<E, NSEQ, FIN, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
@@ -199,8 +204,8 @@ template <typename R> KSet make_real2() {
   KSet k;
   k.kg.first[0] = launch2_first<R, SRC_KG, false>;
   k.kg.first[1] = launch2_first<R, SRC_KG, true>;
-  k.kg.lanczos[0] = launch2_lanczos<R, 2, false>;
-  k.kg.lanczos[1] = launch2_lanczos<R, 2, true>;
+  k.kg.lanczos[0] = launch2_lanczos1<R, false>;
+  k.kg.lanczos[1] = launch2_lanczos1<R, true>;
   k.kg.final_[0] = launch2_final<R, 2, FIN_KG, false>;
   k.kg.final_[1] = launch2_final<R, 2, FIN_KG, true>;
   k.sv[0] = launch2_sv<R, false>;
@@ -214,20 +219,20 @@ template <typename E> KSet make_cplx2() {
   KSet k;
   k.ss2.first[0] = launch2_first<E, SRC_SS2, false>;
   k.ss2.first[1] = launch2_first<E, SRC_SS2, true>;
-  k.ss2.lanczos[0] = launch2_lanczos<E, 1, false>;
-  k.ss2.lanczos[1] = launch2_lanczos<E, 1, true>;
+  k.ss2.lanczos[0] = launch2_lanczos1<E, false>;
+  k.ss2.lanczos[1] = launch2_lanczos1<E, true>;
   k.ss2.final_[0] = launch2_final<E, 1, FIN_SS2, false>;
   k.ss2.final_[1] = launch2_final<E, 1, FIN_SS2, true>;
   k.sewi_a.first[0] = launch2_first<E, SRC_SEWI_A, false>;
   k.sewi_a.first[1] = launch2_first<E, SRC_SEWI_A, true>;
-  k.sewi_a.lanczos[0] = launch2_lanczos<E, 2, false>;
-  k.sewi_a.lanczos[1] = launch2_lanczos<E, 2, true>;
+  k.sewi_a.lanczos[0] = launch2_lanczos1<E, false>;
+  k.sewi_a.lanczos[1] = launch2_lanczos1<E, true>;
   k.sewi_a.final_[0] = launch2_final<E, 2, FIN_SEWI_A, false>;
   k.sewi_a.final_[1] = launch2_final<E, 2, FIN_SEWI_A, true>;
   k.sewi_b.first[0] = launch2_first<E, SRC_SEWI_B, false>;
   k.sewi_b.first[1] = launch2_first<E, SRC_SEWI_B, true>;
-  k.sewi_b.lanczos[0] = launch2_lanczos<E, 1, false>;
-  k.sewi_b.lanczos[1] = launch2_lanczos<E, 1, true>;
+  k.sewi_b.lanczos[0] = launch2_lanczos1<E, false>;
+  k.sewi_b.lanczos[1] = launch2_lanczos1<E, true>;
   k.sewi_b.final_[0] = launch2_final<E, 1, FIN_SEWI_B, false>;
   k.sewi_b.final_[1] = launch2_final<E, 1, FIN_SEWI_B, true>;
   k.ftri = launch_ftri<E>;
@@ -314,6 +319,12 @@ struct TileSet {
   int nlist = 0;
   std::vector<TileDesc> tiles;
   std::vector<int> list;
+  // 2-D Lanczos passes: one section of `live` tiles per Krylov sequence
+  TileDesc *d_lt = nullptr;
+  int *d_nlt1 = nullptr, *d_nlt2 = nullptr;
+  int lcap = 0;
+  int lt_count2 = 0;  // host copy of 2 * live (source of the async upload)
+  std::vector<TileDesc> lt;
 };
 
 }  // namespace
@@ -349,6 +360,7 @@ struct nls_pool {
   cudaGraphExec_t gexec = nullptr;
   int graph_tiles = -1, graph_ring = -1, graph_hc = -1;
   void *graph_part = nullptr;
+  int graph_lcap = -1;
   int step_hc = 0;  // some stepped slot carries a c field
   int ring_blocks = 1;
   int kernels_per_step = 0;
@@ -392,7 +404,8 @@ void pool_free_device(nls_pool *P) {
                   P->c,    P->V,    P->snap,  P->part, P->d_slots, P->d_state, P->d_scal,
                   P->d_beta0, P->d_coef, P->d_ticket, P->main.d_tiles, P->main.d_ntiles, P->main.d_list,
                   P->main.d_nlist, P->first.d_tiles, P->first.d_ntiles, P->first.d_list,
-                  P->first.d_nlist};
+                  P->first.d_nlist, P->main.d_lt, P->main.d_nlt1, P->main.d_nlt2,
+                  P->first.d_lt, P->first.d_nlt1, P->first.d_nlt2};
   for (void *b : bufs)
     if (b) cudaFree(b);
 }
@@ -410,8 +423,9 @@ void slot_tiles(const nls_pool *P, int slot, const SlotDesc &s, std::vector<Tile
   int local = 0;
   if (P->dim == 2) {
     const int N = (int)(16 / P->esz);
+    const int wmax = N == 1 ? HaloLanes<1>::WMAX : HaloLanes<2>::WMAX;
     const int nvec = (s.nx + N - 1) / N;
-    const int nseg = (nvec + 29) / 30;
+    const int nseg = (nvec + wmax - 1) / wmax;
     const int W = (nvec + nseg - 1) / nseg;
     for (int p0 = 0; p0 < s.ny; p0 += P->seg2)
       for (int g = 0; g < nseg; ++g) {
@@ -494,12 +508,30 @@ int rebuild_tables(nls_pool *P) {
     T->nlist = (int)T->list.size();
     int rc = ensure_tiles(P, *T, std::max(T->live, 1));
     if (rc) return rc;
+    T->lt.clear();
+    for (int sq = 0; sq < 2; ++sq)
+      for (const TileDesc &t0 : T->tiles) {
+        TileDesc t1 = t0;
+        t1.local = 2 * t0.local + sq;
+        T->lt.push_back(t1);
+      }
+    if ((int)T->lt.size() > T->lcap || !T->d_lt) {
+      if (T->d_lt) cudaFree(T->d_lt);
+      T->d_lt = nullptr;
+      T->lcap = std::max(2 * T->cap, 128);
+      CK(cudaMalloc(&T->d_lt, sizeof(TileDesc) * T->lcap));
+    }
+    const int n2 = 2 * T->live;
+    T->lt_count2 = n2;
+    if (T->live) CK(cudaMemcpyAsync(T->d_lt, T->lt.data(), sizeof(TileDesc) * n2, cudaMemcpyHostToDevice, P->stream));
+    CK(cudaMemcpyAsync(T->d_nlt1, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+    CK(cudaMemcpyAsync(T->d_nlt2, &T->lt_count2, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     if (T->live) CK(cudaMemcpyAsync(T->d_tiles, T->tiles.data(), sizeof(TileDesc) * T->live, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_ntiles, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     if (T->nlist) CK(cudaMemcpyAsync(T->d_list, T->list.data(), sizeof(int) * T->nlist, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlist, &T->nlist, sizeof(int), cudaMemcpyHostToDevice, P->stream));
   }
-  int rc = ensure_partials(P, std::max(P->main.cap, P->first.cap));
+  int rc = ensure_partials(P, std::max(P->main.lcap, P->first.lcap));
   if (rc) return rc;
   CK(cudaMemcpyAsync(P->d_slots, P->sd.data(), sizeof(SlotDesc) * P->max_slots, cudaMemcpyHostToDevice, P->stream));
   // the pageable sources above are staged by the runtime before returning;
@@ -548,9 +580,17 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
   const int grid = T.cap, hc = P->step_hc;
   CK(L.first[hc](a, grid, P->stream));
   ++nk;
+  StepArgs b = a;  // 2-D passes: one warp per (strip, sequence)
+  int lgrid = grid;
+  if (P->dim == 2) {
+    b.tiles = T.d_lt;
+    b.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
+    b.lt_stride = T.d_nlt1;
+    lgrid = T.lcap;
+  }
   for (int j = 1; j <= P->k - 2; ++j) {
-    a.j = j;
-    CK(L.lanczos[hc](a, grid, P->stream));
+    b.j = j;
+    CK(L.lanczos[hc](b, lgrid, P->stream));
     ++nk;
   }
   CK(P->ks.ftri(a, P->max_slots, P->stream));
@@ -623,7 +663,8 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
 int run_main_step(nls_pool *P) {
   if (!P->use_graph) return enqueue_step(P, P->main, false);
   if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks ||
-      P->graph_hc != P->step_hc || P->graph_part != (void *)P->part) {
+      P->graph_hc != P->step_hc || P->graph_part != (void *)P->part ||
+      P->graph_lcap != P->main.lcap) {
     if (P->gexec) {
       cudaGraphExecDestroy(P->gexec);
       P->gexec = nullptr;
@@ -644,6 +685,7 @@ int run_main_step(nls_pool *P) {
     P->graph_ring = P->ring_blocks;
     P->graph_hc = P->step_hc;
     P->graph_part = (void *)P->part;
+    P->graph_lcap = P->main.lcap;
   }
   CK(cudaGraphLaunch(P->gexec, P->stream));
   return NLS_OK;
@@ -721,60 +763,58 @@ int pool_step_once(nls_pool *P) {
   return NLS_OK;
 }
 
+template <typename E>
+cudaError_t launch_admit(const StepArgs &a, int slot, const double *u0, const double *v0,
+                         const double *m, const double *c, int has_v, int has_c, int sewi,
+                         int64_t npad, cudaStream_t st) {
+  const int blocks = (int)std::min<int64_t>((npad + 255) / 256, 4096);
+  k_admit<E><<<blocks, 256, 0, st>>>(a, slot, u0, v0, m, c, has_v, has_c, sewi);
+  return cudaGetLastError();
+}
+
+// Copy the FP64 inputs into stream-ordered device staging (pageable sources are
+// staged by the runtime before each call returns; pinned ones go by DMA) and
+// convert them on the device into the slot's padded layout.
 int upload_slot(nls_pool *P, int s, const double *u0, const double *v0, const double *m,
                 const double *c) {
   SlotHost &h = P->hs[s];
   const nls_problem &p = h.prob;
-  const SlotDesc &d = P->sd[s];
-  const int64_t np = h.npad;
-  const int nx = p.nx, ny = p.ny, nz = p.dim == 3 ? p.nz : 1;
-  const bool f32 = P->prec == NLS_FP32;
+  const int64_t n = h.n;
   const int comps = P->cplx ? 2 : 1;
-  const double dt = p.T / p.nt;
-  std::vector<unsigned char> hi(np * P->esz, 0), lo(np * P->esz, 0), mr(np * P->rsz, 0),
-      cr(np * P->rsz, 0), dd;
-  if (!P->cplx) dd.assign(np * P->rsz, 0);
-  auto put = [&](std::vector<unsigned char> &buf, int64_t e, int comp, double v, bool real_buf) {
-    const int64_t idx = real_buf ? e : e * comps + comp;
-    if (f32)
-      reinterpret_cast<float *>(buf.data())[idx] = (float)v;
-    else
-      reinterpret_cast<double *>(buf.data())[idx] = v;
-  };
-  for (int z = 0; z < nz; ++z)
-    for (int y = 0; y < ny; ++y)
-      for (int x = 0; x < nx; ++x) {
-        const int64_t pt = ((int64_t)z * ny + y) * nx + x;
-        const int64_t e = ((int64_t)z * ny + y) * d.pitch + x;
-        for (int q = 0; q < comps; ++q) {
-          const double u = u0[pt * comps + q];
-          const double uh = f32 ? (double)(float)u : u;
-          put(hi, e, q, uh, false);
-          put(lo, e, q, u - uh, false);
-        }
-        put(mr, e, 0, m[pt], true);
-        put(cr, e, 0, p.has_c ? c[pt] : 1.0, true);
-        if (!P->cplx) {
-          // u_past = u0 - dt v0 (kg_dev.hpp:55-58); d = u0 - u_past
-          const double vv = v0 ? v0[pt] : 0.0;
-          const double up = u0[pt] - dt * vv;
-          put(dd, e, 0, u0[pt] - up, true);
-        }
-      }
-  const int64_t eo = h.off;
-  CK(cudaMemcpyAsync((char *)P->u_hi + eo * P->esz, hi.data(), np * P->esz, cudaMemcpyHostToDevice, P->stream));
-  CK(cudaMemcpyAsync((char *)P->u_lo + eo * P->esz, lo.data(), np * P->esz, cudaMemcpyHostToDevice, P->stream));
-  CK(cudaMemcpyAsync((char *)P->m + eo * P->rsz, mr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
-  CK(cudaMemcpyAsync((char *)P->c + eo * P->rsz, cr.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
-  if (!P->cplx) CK(cudaMemcpyAsync((char *)P->d + eo * P->rsz, dd.data(), np * P->rsz, cudaMemcpyHostToDevice, P->stream));
-  if (P->method == NLS_NLSE_SEWI) {
-    // u_prev <- u0 before the first (Strang) step (nlse_dev.hpp:206-209)
-    CK(cudaMemcpyAsync((char *)P->up_hi + eo * P->esz, (char *)P->u_hi + eo * P->esz, np * P->esz, cudaMemcpyDeviceToDevice, P->stream));
-    CK(cudaMemcpyAsync((char *)P->up_lo + eo * P->esz, (char *)P->u_lo + eo * P->esz, np * P->esz, cudaMemcpyDeviceToDevice, P->stream));
+  const bool has_v = !P->cplx && v0 != nullptr;
+  const size_t bu = sizeof(double) * n * comps, br = sizeof(double) * n;
+  double *stg = nullptr;
+  const size_t total = bu + br * (1 + (has_v ? 1 : 0) + (p.has_c ? 1 : 0));
+  CK(cudaMallocAsync((void **)&stg, total, P->stream));
+  char *q = (char *)stg;
+  double *du = (double *)q;
+  q += bu;
+  double *dm = (double *)q;
+  q += br;
+  double *dv = nullptr, *dc = nullptr;
+  if (has_v) {
+    dv = (double *)q;
+    q += br;
   }
-  SlotState st{1, 1, 0, 0};
-  CK(cudaMemcpyAsync(P->d_state + s, &st, sizeof(SlotState), cudaMemcpyHostToDevice, P->stream));
-  // the host vectors are staged by the runtime before each call returns
+  if (p.has_c) dc = (double *)q;
+  CK(cudaMemcpyAsync(du, u0, bu, cudaMemcpyHostToDevice, P->stream));
+  CK(cudaMemcpyAsync(dm, m, br, cudaMemcpyHostToDevice, P->stream));
+  if (has_v) CK(cudaMemcpyAsync(dv, v0, br, cudaMemcpyHostToDevice, P->stream));
+  if (p.has_c) CK(cudaMemcpyAsync(dc, c, br, cudaMemcpyHostToDevice, P->stream));
+  // the descriptor must be on the device before the conversion kernel reads it
+  CK(cudaMemcpyAsync(P->d_slots + s, &P->sd[s], sizeof(SlotDesc), cudaMemcpyHostToDevice, P->stream));
+  StepArgs a = base_args(P, P->main);
+  const int sewi = P->method == NLS_NLSE_SEWI ? 1 : 0;
+  cudaError_t e;
+  if (!P->cplx)
+    e = P->prec == NLS_FP64 ? launch_admit<double>(a, s, du, dv, dm, dc, has_v, p.has_c, 0, h.npad, P->stream)
+                            : launch_admit<float>(a, s, du, dv, dm, dc, has_v, p.has_c, 0, h.npad, P->stream);
+  else
+    e = P->prec == NLS_FP64
+            ? launch_admit<Cx<double>>(a, s, du, dv, dm, dc, 0, p.has_c, sewi, h.npad, P->stream)
+            : launch_admit<Cx<float>>(a, s, du, dv, dm, dc, 0, p.has_c, sewi, h.npad, P->stream);
+  CK(e);
+  CK(cudaFreeAsync(stg, P->stream));
   return NLS_OK;
 }
 
@@ -797,6 +837,17 @@ const char *nls_strerror(int code) {
   case NLS_ERR_IO: return "I/O error";
   }
   return "unknown error";
+}
+
+int nls_host_alloc(int64_t bytes, void **out) {
+  if (!out || bytes <= 0) return fail(NLS_ERR_INVALID_ARG, "bad host allocation request");
+  CK(cudaHostAlloc(out, (size_t)bytes, cudaHostAllocPortable));
+  return NLS_OK;
+}
+
+int nls_host_free(void *ptr) {
+  if (ptr) CK(cudaFreeHost(ptr));
+  return NLS_OK;
 }
 
 int nls_set_device(int32_t device) {
@@ -900,8 +951,10 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_scal, sizeof(LzScal) * max_slots * 2 * KMAX);
   if (!rc) rc = al((void **)&P->d_beta0, sizeof(double) * max_slots * 2);
   if (!rc) rc = al((void **)&P->d_coef, sizeof(FinalCoef) * max_slots * 2);
-  if (!rc) rc = al((void **)&P->d_ticket, sizeof(int) * max_slots);
+  if (!rc) rc = al((void **)&P->d_ticket, sizeof(int) * max_slots * 2);
   for (TileSet *T : {&P->main, &P->first}) {
+    if (!rc) rc = al((void **)&T->d_nlt1, sizeof(int));
+    if (!rc) rc = al((void **)&T->d_nlt2, sizeof(int));
     if (!rc) rc = al((void **)&T->d_ntiles, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlist, sizeof(int));
     if (!rc) rc = al((void **)&T->d_list, sizeof(int) * max_slots);
@@ -917,7 +970,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
     cudaError_t e = cudaMemsetAsync(P->d_state, 0, sizeof(SlotState) * max_slots, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->snap, 0, sizeof(double) * ce * 2 * NF, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->d_coef, 0, sizeof(FinalCoef) * max_slots * 2, P->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(P->d_ticket, 0, sizeof(int) * max_slots, P->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->d_ticket, 0, sizeof(int) * max_slots * 2, P->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
     if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -1164,9 +1217,16 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   const int hc = P->step_hc;
-  CK(L.lanczos[hc](a, P->main.cap, P->stream));  // warm
+  int grid = P->main.cap;
+  if (P->dim == 2) {
+    a.tiles = P->main.d_lt;
+    a.ntiles = a.nseq == 2 ? P->main.d_nlt2 : P->main.d_nlt1;
+    a.lt_stride = P->main.d_nlt1;
+    grid = P->main.lcap;
+  }
+  CK(L.lanczos[hc](a, grid, P->stream));  // warm
   CK(cudaEventRecord(e0, P->stream));
-  for (int i = 0; i < iters; ++i) CK(L.lanczos[hc](a, P->main.cap, P->stream));
+  for (int i = 0; i < iters; ++i) CK(L.lanczos[hc](a, grid, P->stream));
   CK(cudaEventRecord(e1, P->stream));
   CK(cudaEventSynchronize(e1));
   float t = 0.f;

@@ -61,7 +61,8 @@ struct StepArgs {
   double tsc[2][2];      // (re, im) time argument per sequence, in units of the slot's dt
   int has_c;             // any slot with a c field
   int sv_pingpong;       // SV step: u_hi / u_alt alternate by step parity
-  int *ticket;           // [slot] arrival counters of the 2-D passes
+  int *ticket;           // [slot][seq] arrival counters of the 2-D passes
+  const int *lt_stride;  // device scalar: tiles per sequence section of the 2-D pass table
   int scal_ready;        // 1: every pass published its scalars (2-D path)
 };
 

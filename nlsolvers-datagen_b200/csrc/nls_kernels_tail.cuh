@@ -385,3 +385,52 @@ __global__ void k_advance(StepArgs a) {
   if (li >= *a.nslot_list) return;
   a.state[a.slot_list[li]].step += 1;
 }
+
+// Admission: FP64 host inputs (staged on the device) -> the slot's padded
+// layout. hi = (R)u, lo = (R)(u - hi) (exactly representable remainder), the
+// KG increment d = u0 - (u0 - dt v0) as kg_dev.hpp:55-58 forms u_past, c = 1
+// where absent, and u_prev = u0 for SEWI (nlse_dev.hpp:206-209). Padding is
+// zero-filled.
+template <typename E>
+__global__ void k_admit(StepArgs a, int slot, const double *u0, const double *v0, const double *m,
+                        const double *c, int has_v, int has_c, int sewi) {
+  using R = typename Traits<E>::R;
+  constexpr int NC = Traits<E>::ncomp;
+  const SlotDesc &s = a.slots[slot];
+  const long long npad = (long long)s.pitch * s.ny * (s.dim == 3 ? s.nz : 1);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < npad;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(e % s.pitch);
+    const long long row = e / s.pitch;  // y + ny z
+    const bool in = x < s.nx;
+    const long long pt = row * s.nx + x;
+    R hi[NC], lo[NC];
+    for (int q = 0; q < NC; ++q) {
+      const double u = in ? u0[pt * NC + q] : 0.0;
+      hi[q] = (R)u;
+      lo[q] = (R)(u - (double)hi[q]);
+    }
+    const long long g = s.off + e;
+    for (int q = 0; q < NC; ++q) {
+      ((R *)a.f.u_hi)[g * NC + q] = hi[q];
+      ((R *)a.f.u_lo)[g * NC + q] = lo[q];
+      if (sewi) {
+        ((R *)a.f.up_hi)[g * NC + q] = hi[q];
+        ((R *)a.f.up_lo)[g * NC + q] = lo[q];
+      }
+    }
+    ((R *)a.f.m)[g] = in ? (R)m[pt] : R(0);
+    ((R *)a.f.c)[g] = in ? (R)(has_c ? c[pt] : 1.0) : R(0);
+    if (NC == 1) {
+      const double u = in ? u0[pt] : 0.0;
+      const double v = (in && has_v) ? v0[pt] : 0.0;
+      const double up = u - s.dt * v;
+      ((R *)a.f.d)[g] = (R)(u - up);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.state[slot].step = 1;
+    a.state[slot].snap = 1;
+    a.state[slot].status = 0;
+  }
+}

@@ -1,8 +1,8 @@
 // 2-D fast path: warp-level row marching. Included inside namespace nlsb.
 //
 // A warp owns a strip of columns [xs, xs + NV*W) of one slot and marches down
-// rows [r0, r1). Lane l (1 <= l <= W) owns the NV consecutive columns starting
-// at xs + NV*(l-1), loaded as one 16-byte vector; lanes 0 and W+1 load the
+// rows [r0, r1). Output lane l owns the NV consecutive columns starting at
+// xs + NV*(l-HL), loaded as one 16-byte vector; HL lanes on each side load the
 // neighbouring vectors as halo. x-neighbours come from warp shuffles, the row
 // window lives in registers and the next rows are prefetched two rows ahead.
 // No shared memory and no block barriers: warps are independent tiles.
@@ -156,17 +156,24 @@ __device__ __forceinline__ void lap_any(const Strip &S, int r, const V16<E> &m, 
 
 // Warp-level tile of a slot.
 // TileDesc of a 2-D warp strip: x0 = first column xs, y0 = output lanes W,
-// [p0, p1) = rows.
+// [p0, p1) = rows. HL halo lanes on each side: forming v_j one column outside
+// the strip needs the column beyond it, which lies in the same vector when a
+// lane holds >= 2 elements and one more lane out when it holds one.
+template <int N> struct HaloLanes {
+  static constexpr int HL = N == 1 ? 2 : 1;
+  static constexpr int WMAX = 32 - 2 * HL;
+};
 template <int N>
 __device__ __forceinline__ Strip make_strip(const SlotDesc &s, const TileDesc &t, int lane) {
+  constexpr int HL = HaloLanes<N>::HL;
   Strip S;
   S.nx = s.nx;
   S.ny = s.ny;
   S.pitch = s.pitch;
   S.off = s.off;
-  S.col0 = t.x0 + N * (lane - 1);
-  S.lane_in = lane <= t.y0 + 1 && S.col0 + N > 0 && S.col0 < s.nx;
-  S.out_lane = lane >= 1 && lane <= t.y0 && S.col0 < s.nx;
+  S.col0 = t.x0 + N * (lane - HL);
+  S.lane_in = lane < t.y0 + 2 * HL && S.col0 + N > 0 && S.col0 < s.nx;
+  S.out_lane = lane >= HL && lane < HL + t.y0 && S.col0 < s.nx;
   return S;
 }
 
@@ -742,31 +749,37 @@ template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
 };
 
 // y_seq = sum_{q < kv-1} W_q V_q + W_{kv-1} V_{kv-1} + Lam (A V_{kv-1}); V_{kv-1}
-// is marched with a one-row window, the other vectors are read at the row only.
+// is marched with a one-row window, the other vectors are read at the row only,
+// eight at a time so that their loads are in flight together. The coefficients
+// sit in shared memory (one area per warp: the warps of a block may belong to
+// different slots).
 template <typename E, int NSEQ, int FIN, bool HC>
 __global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
   using R = typename Traits<E>::R;
+  __shared__ R Wsh[WPB][NSEQ][KMAX][2];
   WARP_TILE_PROLOGUE
   const int kv = a.kv;
   const R opsc = R(a.op_sign * s.inv_h2);
   const R *cf = (const R *)a.f.c;
-  const FinalCoef *FC[NSEQ];
+  const int wib = threadIdx.x >> 5;
   const E *VL[NSEQ];
-  R lr[NSEQ], li[NSEQ], wlr[NSEQ], wli[NSEQ];
+  R lr[NSEQ], li[NSEQ];
 #pragma unroll
   for (int sq = 0; sq < NSEQ; ++sq) {
-    FC[sq] = a.coef + t.slot * 2 + sq;
+    const FinalCoef &F = a.coef[t.slot * 2 + sq];
     VL[sq] = (const E *)a.V + (long long)(sq * kv + kv - 1) * a.vstride;
     if constexpr (sizeof(R) == 4) {
-      lr[sq] = FC[sq]->lam32[0];
-      li[sq] = FC[sq]->lam32[1];
+      lr[sq] = F.lam32[0];
+      li[sq] = F.lam32[1];
     } else {
-      lr[sq] = R(FC[sq]->lam_r);
-      li[sq] = R(FC[sq]->lam_i);
+      lr[sq] = R(F.lam_r);
+      li[sq] = R(F.lam_i);
     }
-    wlr[sq] = coef_w<R>(*FC[sq], kv - 1, false);
-    wli[sq] = coef_w<R>(*FC[sq], kv - 1, true);
+    // lanes >= kv store zeros: the batched loop below reads up to 8 entries past kv-2
+    Wsh[wib][sq][lane][0] = lane < kv ? coef_w<R>(F, lane, false) : R(0);
+    Wsh[wib][sq][lane][1] = lane < kv ? coef_w<R>(F, lane, true) : R(0);
   }
+  __syncwarp();
   V16<E> Lm[NSEQ], Lo[NSEQ], Lp[NSEQ], Ln1[NSEQ], Ln2[NSEQ];
   CRow<E> cw[3], cn1, cn2;
   const int r0 = t.p0, r1 = t.p1;
@@ -805,16 +818,23 @@ __global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
       V16<E> z;
       lap_any<E, R, HC>(S, r, Lm[sq], Lo[sq], Lp[sq], cw, opsc, z);
       V16<E> acc;
+      const R wlr = Wsh[wib][sq][kv - 1][0], wli = Wsh[wib][sq][kv - 1][1];
 #pragma unroll
       for (int e = 0; e < V16<E>::N; ++e)
-        acc.v[e] = cfma(wlr[sq], wli[sq], Lo[sq].v[e], cmul(lr[sq], li[sq], z.v[e]));
+        acc.v[e] = cfma(wlr, wli, Lo[sq].v[e], cmul(lr[sq], li[sq], z.v[e]));
       if (S.lane_in) {
         const E *Vb = (const E *)a.V + (long long)(sq * kv) * a.vstride + S.addr(r);
-        for (int q = 0; q < kv - 1; ++q) {
-          const V16<E> vq = ld16(Vb + (long long)q * a.vstride);
-          const R wr = coef_w<R>(*FC[sq], q, false), wi = coef_w<R>(*FC[sq], q, true);
+        for (int q0 = 0; q0 < kv - 1; q0 += 8) {
+          V16<E> vb[8];
 #pragma unroll
-          for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vq.v[e], acc.v[e]);
+          for (int i = 0; i < 8; ++i)
+            vb[i] = q0 + i < kv - 1 ? ld16(Vb + (long long)(q0 + i) * a.vstride) : vzero<E>();
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const R wr = Wsh[wib][sq][q0 + i][0], wi = Wsh[wib][sq][q0 + i][1];
+#pragma unroll
+            for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vb[i].v[e], acc.v[e]);
+          }
         }
       }
       vmask(acc, S, r);
@@ -900,6 +920,176 @@ __global__ void __launch_bounds__(32 * WPB) k2_sv(StepArgs a) {
           SN[s.n + pt] = (double)d.v[q] / s.dt;
         }
       }
+    }
+  }
+}
+
+// --------------------------------------- Lanczos pass, one sequence per warp
+// Same recurrence as k2_lanczos, but each warp runs one Krylov sequence (the
+// tile table lists every strip once per sequence), which halves the register
+// windows and doubles the warps in flight. With c == 1 the operator uses the
+// zero-filled halo: sum over the four neighbours of (v_nbr - v) plus
+// miss * v, where miss counts the neighbours outside the grid, equals the
+// masked sum over the in-grid neighbours.
+template <typename E, bool HC>
+__global__ void __launch_bounds__(32 * WPB, 4) k2_lanczos1(StepArgs a) {
+  using R = typename Traits<E>::R;
+  constexpr int N = V16<E>::N;
+  constexpr int ND = NDot<E>::value;
+  WARP_TILE_PROLOGUE
+  const int j = a.j, sq = t.local & 1;
+  const R opsc = R(a.op_sign * s.inv_h2);
+  const R *cf = (const R *)a.f.c;
+  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+  const double b0 = a.beta0[t.slot * 2 + sq];
+  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
+  // v_j = cs * lap(V_{j-1}) + ca * V_{j-1} + cb * V_{j-2}
+  const R cs = R(sA * L.inv_b) * opsc;
+  const R car = R(-L.ar * sA * L.inv_b), cai = R(-L.ai * sA * L.inv_b);
+  const R cbr = R(-L.dr * sB * L.inv_b), cbi = R(-L.di * sB * L.inv_b);
+  const R sAr = R(sA);
+  const long long vo = (long long)sq * a.kv;
+  const E *VA = (const E *)a.V + (vo + j - 1) * a.vstride;
+  const E *VB = (const E *)a.V + (vo + (j >= 2 ? j - 2 : 0)) * a.vstride;
+  E *VJ = (E *)a.V + (vo + j) * a.vstride;
+  R xmiss[N];
+  bool xin[N];
+#pragma unroll
+  for (int e = 0; e < N; ++e) {
+    const int x = S.col0 + e;
+    xin[e] = x >= 0 && x < S.nx;
+    xmiss[e] = R((x == 0) + (x == S.nx - 1));
+  }
+  V16<E> A0, A1, A2, An1, An2, An3, B0, Bn1, Bn2, Bn3, Vm, Vo, Vp;
+  CRow<E> cA[3], cn1, cn2, cn3, cV[3];
+  Kahan<R> acc[ND];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) acc[q].init();
+  const int r0 = t.p0, r1 = t.p1;
+  A0 = load_row(VA, S, r0 - 2);
+  A1 = load_row(VA, S, r0 - 1);
+  A2 = load_row(VA, S, r0);
+  An1 = load_row(VA, S, r0 + 1);
+  An2 = load_row(VA, S, r0 + 2);
+  An3 = load_row(VA, S, r0 + 3);
+  if (j >= 2) {
+    B0 = load_row(VB, S, r0 - 1);
+    Bn1 = load_row(VB, S, r0);
+    Bn2 = load_row(VB, S, r0 + 1);
+    Bn3 = load_row(VB, S, r0 + 2);
+  } else {
+    B0 = Bn1 = Bn2 = Bn3 = vzero<E>();
+  }
+  Vo = vzero<E>();
+  Vp = vzero<E>();
+  if constexpr (HC) {
+    cA[0] = load_crow<E>(cf, S, r0 - 2);
+    cA[1] = load_crow<E>(cf, S, r0 - 1);
+    cA[2] = load_crow<E>(cf, S, r0);
+    cn1 = load_crow<E>(cf, S, r0 + 1);
+    cn2 = load_crow<E>(cf, S, r0 + 2);
+    cn3 = load_crow<E>(cf, S, r0 + 3);
+    cV[0] = cV[1] = cV[2] = cA[0];  // rotated in before the first use
+  }
+  for (int r = r0 - 2; r < r1; ++r) {
+    const int q = r + 1;
+    // (a) v_j on row q
+    {
+      V16<E> v;
+      if constexpr (HC) {
+        V16<E> w;
+        lap_any<E, R, true>(S, q, A0, A1, A2, cA, R(1), w);
+#pragma unroll
+        for (int e = 0; e < N; ++e) v.v[e] = cfma(cbr, cbi, B0.v[e], cfma(car, cai, A1.v[e], scale(w.v[e], cs)));
+      } else {
+        const E lft = shfl_up1(A1.v[N - 1]);
+        const E rgt = shfl_dn1(A1.v[0]);
+        const R rmiss = R((q == 0) + (q == S.ny - 1));
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+          const E c = A1.v[e];
+          const E xl = e == 0 ? lft : A1.v[e - 1];
+          const E xr = e == N - 1 ? rgt : A1.v[e + 1];
+          E acc4 = add(add(sub(xl, c), sub(xr, c)), add(sub(A0.v[e], c), sub(A2.v[e], c)));
+          acc4 = fma_s(xmiss[e] + rmiss, c, acc4);
+          v.v[e] = cfma(cbr, cbi, B0.v[e], cfma(car, cai, c, scale(acc4, cs)));
+        }
+      }
+      const bool rq = q >= 0 && q < S.ny;
+#pragma unroll
+      for (int e = 0; e < N; ++e)
+        if (!(rq && xin[e])) v.v[e] = zero<E>();
+      Vm = Vo;
+      Vo = Vp;
+      Vp = v;
+      if (S.out_lane && q >= r0 && q < r1) st16(VJ + S.addr(q), v);
+    }
+    if constexpr (HC) {
+      cV[0] = cV[1];
+      cV[1] = cV[2];
+      cV[2] = cA[1];
+    }
+    // (b) z_j = A v_j on row r, dots with v_j(r) and v_{j-1}(r) = sA * A0
+    if (r >= r0) {
+      V16<E> z;
+      if constexpr (HC) {
+        lap_any<E, R, true>(S, r, Vm, Vo, Vp, cV, opsc, z);
+      } else {
+        const E lft = shfl_up1(Vo.v[N - 1]);
+        const E rgt = shfl_dn1(Vo.v[0]);
+        const R rmiss = R((r == 0) + (r == S.ny - 1));
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+          const E c = Vo.v[e];
+          const E xl = e == 0 ? lft : Vo.v[e - 1];
+          const E xr = e == N - 1 ? rgt : Vo.v[e + 1];
+          E acc4 = add(add(sub(xl, c), sub(xr, c)), add(sub(Vm.v[e], c), sub(Vp.v[e], c)));
+          acc4 = fma_s(xmiss[e] + rmiss, c, acc4);
+          z.v[e] = scale(acc4, opsc);
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < N; ++e)
+        if (!xin[e]) z.v[e] = zero<E>();
+      if (S.out_lane) dots_row(acc, z, Vo, vscale(A0, sAr));
+    }
+    // (c) shift and prefetch three rows ahead
+    A0 = A1;
+    A1 = A2;
+    A2 = An1;
+    An1 = An2;
+    An2 = An3;
+    An3 = load_row(VA, S, q + 5);
+    B0 = Bn1;
+    Bn1 = Bn2;
+    Bn2 = Bn3;
+    Bn3 = j >= 2 ? load_row(VB, S, q + 4) : vzero<E>();
+    if constexpr (HC) {
+      cA[0] = cA[1];
+      cA[1] = cA[2];
+      cA[2] = cn1;
+      cn1 = cn2;
+      cn2 = cn3;
+      cn3 = load_crow<E>(cf, S, q + 5);
+    }
+  }
+  double vals[ND];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) vals[q] = S.out_lane ? acc[q].val() : 0.0;
+  // the table has one section of TT tiles per sequence, each in slot order:
+  // the tiles of (slot, sq) are [sq * TT + tile_begin, + tile_count)
+  const int tc = s.tile_count, TT = *a.lt_stride;
+  if (warp_publish<ND>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot * 2 + sq,
+                       tc, lane)) {
+    const double *part = a.part + (long long)j * a.part_stride;
+    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin, tc, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<Traits<E>::cplx>(tv, Eps<R>::v);
+      a.ticket[t.slot * 2 + sq] = 0;
     }
   }
 }

@@ -31,7 +31,7 @@ SYMBOLS = [
     "nls_pool_poll", "nls_pool_release", "nls_pool_sync", "nls_pool_usage",
     "nls_pool_set_graphs", "nls_pool_set_segment", "nls_pool_time_pass",
     "nls_pool_kernels_per_step", "nls_pool_destroy", "nls_strerror", "nls_last_error",
-    "nls_pool_step_timed", "nls_set_device",
+    "nls_pool_step_timed", "nls_set_device", "nls_host_alloc", "nls_host_free",
 ]
 
 
@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
         "nls_pool_step_timed": [vp, i32, ctypes.POINTER(ctypes.c_float)],
         "nls_pool_destroy": [vp],
         "nls_set_device": [i32],
+        "nls_host_alloc": [i64, ctypes.POINTER(vp)],
+        "nls_host_free": [vp],
         "nls_last_error": [ctypes.c_char_p, i32],
     }
     for name, args in sig.items():

@@ -99,6 +99,18 @@ def reference_phi4_rm(spec: Spec) -> float:
     return -(0.01 * math.sqrt(2.0 * dx) / spec.dt)
 
 
+def pinned_empty(shape, dtype=np.float64):
+    """numpy array in page-locked host memory (freed with the array)."""
+    import weakref
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    ptr = ctypes.c_void_p()
+    check(lib().nls_host_alloc(max(nbytes, 1), ctypes.byref(ptr)))
+    buf = (ctypes.c_char * max(nbytes, 1)).from_address(ptr.value)
+    weakref.finalize(buf, lib().nls_host_free, ctypes.c_void_p(ptr.value))
+    return np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+
+
 def _dptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -258,5 +270,5 @@ class Pool:
             pass
 
 
-__all__ = ["Spec", "Solver", "Pool", "NlsError", "KG_GAUTSCHI", "KG_SV", "SP4_SV",
+__all__ = ["Spec", "Solver", "Pool", "NlsError", "pinned_empty", "KG_GAUTSCHI", "KG_SV", "SP4_SV",
            "SP4_GAUTSCHI", "NLSE_SS2", "NLSE_SEWI", "FP32", "FP64", "reference_phi4_rm"]

@@ -122,6 +122,23 @@ def test_nlse_sewi(prec, variant):
     _check(spec, u0, None, m, c, TOL64 if prec == "fp64" else TOL32)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("kind", ["kg", "sv", "nlse"])
+def test_multi_strip_wide_grid(prec, kind):
+    """Grids wider than one warp strip (120 float / 60 double or complex-float /
+    28 complex-double columns) exercise the strip halos and the slot reduction
+    over many tiles."""
+    W, FP32, FP64, KG, KG_SV, *rest = _cases()
+    p = FP64 if prec == "fp64" else FP32
+    if kind == "nlse":
+        spec, u0, v0, m, c = W.nlse_case(131, 10.0, T=0.02, nt=20, ns=4, k=10, seed=9, precision=p)
+    else:
+        spec, u0, v0, m, c = W.kg_case(131, 10.0, T=0.2, nt=20, ns=4, k=10, seed=9, precision=p,
+                                       method=KG if kind == "kg" else KG_SV)
+    _check(spec, u0, v0, m, c, TOL64 if prec == "fp64" else TOL32,
+           vel_tol=1e-9 if prec == "fp64" else 1e-4)
+
+
 def test_batch_alone_equals_mixed():
     """Each trajectory's tiling and reduction order depend only on itself:
     results are bitwise identical alone and inside a batch of uneven sizes."""
