@@ -223,13 +223,13 @@ def run_reference(args, ws, rank):
 
 
 def run_small(args, lrank):
-    """--small: 16 trajectories of the same workload (k=10, 32-row segments),
-    warmup + steps only; the case the ncu captures profile (~0.2 GB on the GPU,
-    above the 126 MB L2)."""
+    """--small: --batch trajectories (default 16) of the same workload (k=10,
+    32-row segments), warmup + steps only; the case the ncu captures profile
+    (16: ~0.2 GB, 64: ~0.7 GB on the GPU, both above the 126 MB L2)."""
     import nlsb200 as nl
     from nlsb200.solver import FP32, KG_GAUTSCHI, Pool
     nl.lib().nls_set_device(lrank)
-    B, k = 16, 10
+    B, k = args.batch, 10
     cases = make_batch(B, 0, k)
     cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
     pool = Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=32)
@@ -360,7 +360,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--small", action="store_true",
-                    help="16-trajectory profiling case (no autotune, e2e or CPU leg)")
+                    help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
+    ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

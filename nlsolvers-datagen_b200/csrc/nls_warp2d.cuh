@@ -618,22 +618,28 @@ template <int FIN, typename E> struct FinRow;
 template <typename R> struct FinRow<FIN_KG, R> {
   // Gautschi (kg_single.cuh:101-126) with d = u - u_past:
   // d+ = d + 2 (cos(tau sqrt A) - I) u + tau^2 sinc^2(tau sqrt A) g(u), u+ = u + d+.
+  struct Fld {
+    V16<R> hi, lo, d;
+  };
+  static __device__ __forceinline__ Fld load(const StepArgs &a, const Strip &S, int r) {
+    const long long o = S.addr(r);
+    return Fld{ld16((const R *)a.f.u_hi + o), ld16((const R *)a.f.u_lo + o), ld16((const R *)a.f.d + o)};
+  }
   static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
-                                               int step, int r, const V16<R> *y) {
+                                               int step, int r, Fld f, const V16<R> *y) {
     constexpr int N = V16<R>::N;
-    R *uh = (R *)a.f.u_hi + S.addr(r), *ul = (R *)a.f.u_lo + S.addr(r), *dd = (R *)a.f.d + S.addr(r);
-    V16<R> hi = ld16((const R *)uh), lo = ld16((const R *)ul), d = ld16((const R *)dd);
+    const long long o = S.addr(r);
     const R dt = R(s.dt), t2 = dt * dt;
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-      const R dp = d.v[q] + R(2) * y[0].v[q] + t2 * y[1].v[q];
-      comp_add(hi.v[q], lo.v[q], dp);
-      d.v[q] = dp;
+      const R dp = f.d.v[q] + R(2) * y[0].v[q] + t2 * y[1].v[q];
+      comp_add(f.hi.v[q], f.lo.v[q], dp);
+      f.d.v[q] = dp;
     }
-    vmask(d, S, r);
-    st16(uh, hi);
-    st16(ul, lo);
-    st16(dd, d);
+    vmask(f.d, S, r);
+    st16((R *)a.f.u_hi + o, f.hi);
+    st16((R *)a.f.u_lo + o, f.lo);
+    st16((R *)a.f.d + o, f.d);
     int fr;
     if (snap_step(s, step, fr)) {
       double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
@@ -642,8 +648,8 @@ template <typename R> struct FinRow<FIN_KG, R> {
         const int x = S.col0 + q;
         if (x >= 0 && x < S.nx) {
           const long long pt = (long long)r * S.nx + x;
-          SN[pt] = (double)hi.v[q] + (double)lo.v[q];
-          SN[s.n + pt] = (double)d.v[q] / s.dt;
+          SN[pt] = (double)f.hi.v[q] + (double)f.lo.v[q];
+          SN[s.n + pt] = (double)f.d.v[q] / s.dt;
         }
       }
     }
@@ -653,25 +659,32 @@ template <typename R> struct FinRow<FIN_KG, R> {
 template <typename R> struct FinRow<FIN_SS2, Cx<R>> {
   // u <- N_{tau/2}(e^{i tau L} N_{tau/2}(u)) accumulated as u += D1 + I + D2
   // (nlse_dev.hpp:187-203), D1 = u(e^{i phi1}-1), D2 = w(e^{i phi2}-1), w = N(u)+I.
+  struct Fld {
+    V16<Cx<R>> hi, lo;
+    CRow<Cx<R>> m;
+  };
+  static __device__ __forceinline__ Fld load(const StepArgs &a, const Strip &S, int r) {
+    const long long o = S.addr(r);
+    return Fld{ld16((const Cx<R> *)a.f.u_hi + o), ld16((const Cx<R> *)a.f.u_lo + o),
+               load_crow<Cx<R>>((const R *)a.f.m, S, r)};
+  }
   static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
-                                               int step, int r, const V16<Cx<R>> *y) {
+                                               int step, int r, Fld f, const V16<Cx<R>> *y) {
     constexpr int N = V16<Cx<R>>::N;
-    Cx<R> *uh = (Cx<R> *)a.f.u_hi + S.addr(r), *ul = (Cx<R> *)a.f.u_lo + S.addr(r);
-    V16<Cx<R>> hi = ld16((const Cx<R> *)uh), lo = ld16((const Cx<R> *)ul);
-    const CRow<Cx<R>> m = load_crow<Cx<R>>((const R *)a.f.m, S, r);
+    const long long o = S.addr(r);
     const R half = R(0.5 * s.dt);
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-      const R kap = R(s.p3) * m.v[q] + R(s.q3);
-      const Cx<R> d1 = cexpm1_mul(hi.v[q], half * (kap * norm2(hi.v[q])));
-      const Cx<R> w = add(add(hi.v[q], d1), y[0].v[q]);
+      const R kap = R(s.p3) * f.m.v[q] + R(s.q3);
+      const Cx<R> d1 = cexpm1_mul(f.hi.v[q], half * (kap * norm2(f.hi.v[q])));
+      const Cx<R> w = add(add(f.hi.v[q], d1), y[0].v[q]);
       const Cx<R> d2 = cexpm1_mul(w, half * (kap * norm2(w)));
-      comp_add(hi.v[q], lo.v[q], add(add(d1, y[0].v[q]), d2));
+      comp_add(f.hi.v[q], f.lo.v[q], add(add(d1, y[0].v[q]), d2));
     }
-    vmask(hi, S, r);
-    vmask(lo, S, r);
-    st16(uh, hi);
-    st16(ul, lo);
+    vmask(f.hi, S, r);
+    vmask(f.lo, S, r);
+    st16((Cx<R> *)a.f.u_hi + o, f.hi);
+    st16((Cx<R> *)a.f.u_lo + o, f.lo);
     int fr;
     if (snap_step(s, step, fr)) {
       double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
@@ -680,8 +693,8 @@ template <typename R> struct FinRow<FIN_SS2, Cx<R>> {
         const int x = S.col0 + q;
         if (x >= 0 && x < S.nx) {
           const long long pt = (long long)r * S.nx + x;
-          SN[2 * pt] = (double)hi.v[q].x + (double)lo.v[q].x;
-          SN[2 * pt + 1] = (double)hi.v[q].y + (double)lo.v[q].y;
+          SN[2 * pt] = (double)f.hi.v[q].x + (double)f.lo.v[q].x;
+          SN[2 * pt + 1] = (double)f.hi.v[q].y + (double)f.lo.v[q].y;
         }
       }
     }
@@ -690,8 +703,10 @@ template <typename R> struct FinRow<FIN_SS2, Cx<R>> {
 
 template <typename R> struct FinRow<FIN_SEWI_A, Cx<R>> {
   // y_a = sinc(tau L) B(u), I2 = (e^{2 i tau L} - I) u_prev (nlse_dev.hpp:215-223)
+  struct Fld {};
+  static __device__ __forceinline__ Fld load(const StepArgs &, const Strip &, int) { return Fld{}; }
   static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &, const Strip &S, int,
-                                               int r, const V16<Cx<R>> *y) {
+                                               int r, Fld, const V16<Cx<R>> *y) {
     st16((Cx<R> *)a.f.ya + S.addr(r), y[0]);
     st16((Cx<R> *)a.f.ib + S.addr(r), y[1]);
   }
@@ -700,21 +715,26 @@ template <typename R> struct FinRow<FIN_SEWI_A, Cx<R>> {
 template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
   // y_b = e^{i tau L} y_a, y_2 = u_prev + I2; u+ = y_b - 2 i tau y_2 (reference
   // operand order, nlse_dev.hpp:54-64 called at :225) or y_2 - 2 i tau y_b.
+  struct Fld {
+    V16<Cx<R>> i2, uh, ul, ph, pl;
+  };
+  static __device__ __forceinline__ Fld load(const StepArgs &a, const Strip &S, int r) {
+    const long long o = S.addr(r);
+    return Fld{ld16((const Cx<R> *)a.f.ib + o), ld16((const Cx<R> *)a.f.u_hi + o),
+               ld16((const Cx<R> *)a.f.u_lo + o), ld16((const Cx<R> *)a.f.up_hi + o),
+               ld16((const Cx<R> *)a.f.up_lo + o)};
+  }
   static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
-                                               int step, int r, const V16<Cx<R>> *y) {
+                                               int step, int r, Fld f, const V16<Cx<R>> *y) {
     constexpr int N = V16<Cx<R>>::N;
     const long long o = S.addr(r);
-    Cx<R> *uh = (Cx<R> *)a.f.u_hi + o, *ul = (Cx<R> *)a.f.u_lo + o;
-    Cx<R> *ph = (Cx<R> *)a.f.up_hi + o, *pl = (Cx<R> *)a.f.up_lo + o;
-    const V16<Cx<R>> i2 = ld16((const Cx<R> *)a.f.ib + o);
-    const V16<Cx<R>> uh0 = ld16((const Cx<R> *)uh), ul0 = ld16((const Cx<R> *)ul);
-    V16<Cx<R>> nh = ld16((const Cx<R> *)ph), nl = ld16((const Cx<R> *)pl);
+    V16<Cx<R>> nh = f.ph, nl = f.pl;
     const R tt = R(2.0 * s.dt);
 #pragma unroll
     for (int q = 0; q < N; ++q) {
       const Cx<R> yb = y[0].v[q];
       if (s.variant == 0) {
-        const Cx<R> y2 = add(nh.v[q], i2.v[q]);
+        const Cx<R> y2 = add(nh.v[q], f.i2.v[q]);
         const Cx<R> h = Cx<R>{yb.x + tt * y2.y, yb.y - tt * y2.x};
         const Cx<R> l = Cx<R>{tt * nl.v[q].y, -tt * nl.v[q].x};
         R sx, ex, sy, ey;
@@ -723,15 +743,15 @@ template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
         nh.v[q] = Cx<R>{sx, sy};
         nl.v[q] = Cx<R>{ex, ey};
       } else {
-        comp_add(nh.v[q], nl.v[q], Cx<R>{i2.v[q].x + tt * yb.y, i2.v[q].y - tt * yb.x});
+        comp_add(nh.v[q], nl.v[q], Cx<R>{f.i2.v[q].x + tt * yb.y, f.i2.v[q].y - tt * yb.x});
       }
     }
     vmask(nh, S, r);
     vmask(nl, S, r);
-    st16(ph, uh0);
-    st16(pl, ul0);
-    st16(uh, nh);
-    st16(ul, nl);
+    st16((Cx<R> *)a.f.up_hi + o, f.uh);
+    st16((Cx<R> *)a.f.up_lo + o, f.ul);
+    st16((Cx<R> *)a.f.u_hi + o, nh);
+    st16((Cx<R> *)a.f.u_lo + o, nl);
     int fr;
     if (snap_step(s, step, fr)) {
       double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
@@ -748,14 +768,17 @@ template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
   }
 };
 
-// y_seq = sum_{q < kv-1} W_q V_q + W_{kv-1} V_{kv-1} + Lam (A V_{kv-1}); V_{kv-1}
-// is marched with a one-row window, the other vectors are read at the row only,
-// eight at a time so that their loads are in flight together. The coefficients
-// sit in shared memory (one area per warp: the warps of a block may belong to
-// different slots).
+// y_seq = sum_{q < kv-1} W_q V_q + W_{kv-1} V_{kv-1} + Lam (A V_{kv-1}). Every
+// load of a row (the next row of V_{kv-1}, the first eight vectors V_q of each
+// sequence and the integrator's fields) is issued before any arithmetic, so a
+// row costs one memory round trip; vectors past the first eight (k > 9) follow
+// in further batches. Coefficients sit in shared memory, one area per warp
+// (the warps of a block may belong to different slots).
 template <typename E, int NSEQ, int FIN, bool HC>
 __global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
   using R = typename Traits<E>::R;
+  using FR = FinRow<FIN, E>;
+  constexpr int NB = 8;
   __shared__ R Wsh[WPB][NSEQ][KMAX][2];
   WARP_TILE_PROLOGUE
   const int kv = a.kv;
@@ -775,44 +798,57 @@ __global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
       lr[sq] = R(F.lam_r);
       li[sq] = R(F.lam_i);
     }
-    // lanes >= kv store zeros: the batched loop below reads up to 8 entries past kv-2
+    // lanes >= kv store zeros: the batched loop reads up to NB entries past kv-2
     Wsh[wib][sq][lane][0] = lane < kv ? coef_w<R>(F, lane, false) : R(0);
     Wsh[wib][sq][lane][1] = lane < kv ? coef_w<R>(F, lane, true) : R(0);
   }
   __syncwarp();
-  V16<E> Lm[NSEQ], Lo[NSEQ], Lp[NSEQ], Ln1[NSEQ], Ln2[NSEQ];
-  CRow<E> cw[3], cn1, cn2;
+  const bool io = S.out_lane;
+  V16<E> Lm[NSEQ], Lo[NSEQ], Lp[NSEQ], Ln1[NSEQ];
+  CRow<E> cw[3], cn1;
   const int r0 = t.p0, r1 = t.p1;
 #pragma unroll
   for (int sq = 0; sq < NSEQ; ++sq) {
     Lo[sq] = load_row(VL[sq], S, r0 - 1);
     Lp[sq] = load_row(VL[sq], S, r0);
     Ln1[sq] = load_row(VL[sq], S, r0 + 1);
-    Ln2[sq] = load_row(VL[sq], S, r0 + 2);
   }
   if constexpr (HC) {
     cw[1] = load_crow<E>(cf, S, r0 - 1);
     cw[2] = load_crow<E>(cf, S, r0);
     cn1 = load_crow<E>(cf, S, r0 + 1);
-    cn2 = load_crow<E>(cf, S, r0 + 2);
   }
   for (int r = r0; r < r1; ++r) {
-    V16<E> y[NSEQ];
+    // ---- issue the row's loads
+    V16<E> Ln2[NSEQ];
+    V16<E> vb[NSEQ][NB];
+    CRow<E> cn2;
+#pragma unroll
+    for (int sq = 0; sq < NSEQ; ++sq) {
+      Ln2[sq] = load_row(VL[sq], S, r + 2);
+      const E *Vb = (const E *)a.V + (long long)(sq * kv) * a.vstride + S.addr(r);
+#pragma unroll
+      for (int i = 0; i < NB; ++i)
+        vb[sq][i] = (io && i < kv - 1) ? ld16(Vb + (long long)i * a.vstride) : vzero<E>();
+    }
+    if constexpr (HC) cn2 = load_crow<E>(cf, S, r + 2);
+    typename FR::Fld fld;
+    if (io) fld = FR::load(a, S, r);
+    // ---- arithmetic
 #pragma unroll
     for (int sq = 0; sq < NSEQ; ++sq) {
       Lm[sq] = Lo[sq];
       Lo[sq] = Lp[sq];
       Lp[sq] = Ln1[sq];
       Ln1[sq] = Ln2[sq];
-      Ln2[sq] = load_row(VL[sq], S, r + 3);
     }
     if constexpr (HC) {
       cw[0] = cw[1];
       cw[1] = cw[2];
       cw[2] = cn1;
       cn1 = cn2;
-      cn2 = load_crow<E>(cf, S, r + 3);
     }
+    V16<E> y[NSEQ];
 #pragma unroll
     for (int sq = 0; sq < NSEQ; ++sq) {
       V16<E> z;
@@ -822,25 +858,31 @@ __global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
 #pragma unroll
       for (int e = 0; e < V16<E>::N; ++e)
         acc.v[e] = cfma(wlr, wli, Lo[sq].v[e], cmul(lr[sq], li[sq], z.v[e]));
-      if (S.lane_in) {
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        const R wr = Wsh[wib][sq][i][0], wi = Wsh[wib][sq][i][1];
+#pragma unroll
+        for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vb[sq][i].v[e], acc.v[e]);
+      }
+      if (io && kv - 1 > NB) {
         const E *Vb = (const E *)a.V + (long long)(sq * kv) * a.vstride + S.addr(r);
-        for (int q0 = 0; q0 < kv - 1; q0 += 8) {
-          V16<E> vb[8];
+        for (int q0 = NB; q0 < kv - 1; q0 += NB) {
+          V16<E> vx[NB];
 #pragma unroll
-          for (int i = 0; i < 8; ++i)
-            vb[i] = q0 + i < kv - 1 ? ld16(Vb + (long long)(q0 + i) * a.vstride) : vzero<E>();
+          for (int i = 0; i < NB; ++i)
+            vx[i] = q0 + i < kv - 1 ? ld16(Vb + (long long)(q0 + i) * a.vstride) : vzero<E>();
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
+          for (int i = 0; i < NB; ++i) {
             const R wr = Wsh[wib][sq][q0 + i][0], wi = Wsh[wib][sq][q0 + i][1];
 #pragma unroll
-            for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vb[i].v[e], acc.v[e]);
+            for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vx[i].v[e], acc.v[e]);
           }
         }
       }
       vmask(acc, S, r);
       y[sq] = acc;
     }
-    if (S.out_lane && S.row_ok(r)) FinRow<FIN, E>::apply(a, s, S, step, r, y);
+    if (io && S.row_ok(r)) FR::apply(a, s, S, step, r, fld, y);
   }
 }
 
