@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -93,6 +94,22 @@ cudaError_t launch2_lanczos(const StepArgs &a, int tiles, cudaStream_t st) {
 template <typename E, bool HC>
 cudaError_t launch2_lanczos1(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_lanczos1<E, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
+// Blocks per SM the packed FP32 pass is compiled for (register cap 128 or 168);
+// NLS_F32_BLOCKS=3 selects the 168-register build.
+int f32_minb() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_F32_BLOCKS");
+    return (e && std::atoi(e) == 3) ? 3 : 4;
+  }();
+  return v;
+}
+cudaError_t launch2_lanczos1_f32(const StepArgs &a, int tiles, cudaStream_t st) {
+  if (f32_minb() == 3)
+    k2_lanczos1_f32<3><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  else
+    k2_lanczos1_f32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
 template <typename E, int NSEQ, int FIN, bool HC>
@@ -206,6 +223,7 @@ template <typename R> KSet make_real2() {
   k.kg.first[1] = launch2_first<R, SRC_KG, true>;
   k.kg.lanczos[0] = launch2_lanczos1<R, false>;
   k.kg.lanczos[1] = launch2_lanczos1<R, true>;
+  if constexpr (sizeof(R) == 4) k.kg.lanczos[0] = launch2_lanczos1_f32;  // packed FP32x2 path
   k.kg.final_[0] = launch2_final<R, 2, FIN_KG, false>;
   k.kg.final_[1] = launch2_final<R, 2, FIN_KG, true>;
   k.sv[0] = launch2_sv<R, false>;

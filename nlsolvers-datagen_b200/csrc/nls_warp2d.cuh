@@ -1135,3 +1135,187 @@ __global__ void __launch_bounds__(32 * WPB, 4) k2_lanczos1(StepArgs a) {
     }
   }
 }
+
+// -------------------------- FP32 Lanczos pass with packed FP32x2 arithmetic
+// The headline path (real FP32 fields, c == 1). Each lane's 16-byte vector is
+// two float2 pairs processed with the sm_100 packed FFMA2 / FADD2 / FMUL2
+// instructions. Masks are multiplicative (no per-element branches), and the
+// row loop is unrolled six times so that the register rings of V_{j-1}
+// (6 rows: 3 live + 3 prefetched), V_{j-2} (3 rows) and v_j (3 rows) rotate
+// by renaming instead of moves. Iterations past the last row are computed on
+// zero rows and discarded.
+struct F4 {
+  float2 a, b;  // elements (0,1), (2,3)
+};
+__device__ __forceinline__ F4 f4_load(const float *p) {
+  const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+  return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+__device__ __forceinline__ void f4_store(float *p, const F4 &v) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v.a.x, v.a.y, v.b.x, v.b.y);
+}
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 add2(float2 x, float2 y) { return __fadd2_rn(x, y); }
+__device__ __forceinline__ float2 mul2(float2 x, float2 y) { return __fmul2_rn(x, y); }
+__device__ __forceinline__ float2 fma2(float2 x, float2 y, float2 z) { return __ffma2_rn(x, y, z); }
+__device__ __forceinline__ float2 neg2(float2 x) { return make_float2(-x.x, -x.y); }
+
+// Row of the count-form operator (differences first): with zero-filled halo,
+// sum_nbr (v_nbr - v) + miss * v equals the masked sum over in-grid neighbours.
+__device__ __forceinline__ F4 lap4(const F4 &m, const F4 &o, const F4 &p, float lft, float rgt,
+                                   const F4 &miss) {
+  const float2 nc0 = neg2(o.a), nc1 = neg2(o.b);
+  // x-neighbours of elements (0,1): (lft, o0) and (o1, o2); of (2,3): (o1, o2) / (o3, rgt)
+  const float2 xl0 = make_float2(lft, o.a.x), xr0 = make_float2(o.a.y, o.b.x);
+  const float2 xl1 = make_float2(o.a.y, o.b.x), xr1 = make_float2(o.b.y, rgt);
+  float2 s0 = add2(add2(xl0, nc0), add2(xr0, nc0));
+  float2 s1 = add2(add2(xl1, nc1), add2(xr1, nc1));
+  s0 = add2(s0, add2(add2(m.a, nc0), add2(p.a, nc0)));
+  s1 = add2(s1, add2(add2(m.b, nc1), add2(p.b, nc1)));
+  return F4{fma2(miss.a, o.a, s0), fma2(miss.b, o.b, s1)};
+}
+
+struct Kahan2 {
+  float2 s, c;
+  __device__ __forceinline__ void init() { s = c = make_float2(0.f, 0.f); }
+  __device__ __forceinline__ void add(float2 v) {
+    const float2 y = add2(v, neg2(c));
+    const float2 t = add2(s, y);
+    c = add2(add2(t, neg2(s)), neg2(y));
+    s = t;
+  }
+  __device__ __forceinline__ double val() const {
+    return ((double)s.x - (double)c.x) + ((double)s.y - (double)c.y);
+  }
+};
+
+template <int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32(StepArgs a) {
+  using E = float;
+  WARP_TILE_PROLOGUE
+  const int j = a.j, sq = t.local & 1;
+  const float opsc = float(a.op_sign * s.inv_h2);
+  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+  const double b0 = a.beta0[t.slot * 2 + sq];
+  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
+  const float2 CS = f2(float(sA * L.inv_b) * opsc), CA = f2(float(-L.ar * sA * L.inv_b)),
+               CB = f2(float(-L.dr * sB * L.inv_b)), SA = f2(float(sA)), OP = f2(opsc);
+  const long long vo = (long long)sq * a.kv;
+  const bool hasB = j >= 2;
+  // per-lane row pointers (advanced by the pitch each row)
+  const long long lane_off = s.off + S.col0;
+  const float *pA = (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
+  const float *pB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
+  float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
+  const long long P = s.pitch;
+  // column masks and missing-neighbour counts of the four elements
+  F4 xval, xmiss;
+  {
+    float v[4], m[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == S.nx - 1));
+    }
+    xval = F4{make_float2(v[0], v[1]), make_float2(v[2], v[3])};
+    xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  const bool ld = S.lane_in, io = S.out_lane;
+  const int r0 = t.p0, r1 = t.p1, ny = S.ny;
+  auto rowA = [&](int r) -> F4 {
+    return (ld && r >= 0 && r < ny) ? f4_load(pA + r * P) : F4{f2(0.f), f2(0.f)};
+  };
+  auto rowB = [&](int r) -> F4 {
+    return (ld && hasB && r >= 0 && r < ny) ? f4_load(pB + r * P) : F4{f2(0.f), f2(0.f)};
+  };
+  Kahan<float> k0, k1, k2, k3, k4, k5;  // <z,v-> <z,v> <v-,v> |z|^2 |v|^2 |v-|^2
+  k0.init(); k1.init(); k2.init(); k3.init(); k4.init(); k5.init();
+  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f), q5 = f2(0.f);
+  int npair = 0;
+  // rings at the first iteration q = r0 - 1: A rows q-1 .. q+4, B rows q .. q+2
+  F4 A0 = rowA(r0 - 2), A1 = rowA(r0 - 1), A2 = rowA(r0), A3 = rowA(r0 + 1), A4 = rowA(r0 + 2),
+     A5 = rowA(r0 + 3);
+  F4 B0 = rowB(r0 - 1), B1 = rowB(r0), B2 = rowB(r0 + 1);
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  F4 V0 = zero4, V1 = zero4, V2 = zero4;
+  const int qb = r0 - 1, qe = r1;  // v_j rows
+  const int nit = ((qe - qb + 1) + 5) / 6 * 6;
+
+  // One row step: Am, Ac, Ap = A rows q-1, q, q+1; Af = register to refill with
+  // A(q+5); Bc = B(q) (refilled with B(q+3)); Vm, Vc = v rows q-2, q-1 and Vn
+  // receives v(q). Then z at row q-1 and its dots.
+#define NLSB_ROW(Am, Ac, Ap, Af, Bc, Vm, Vc, Vn)                                              \
+  {                                                                                           \
+    const int q = qb + it;                                                                    \
+    {                                                                                         \
+      const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
+      const float2 rm = f2(float((q == 0) + (q == ny - 1)));                                  \
+      const F4 miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                               \
+      const F4 w = lap4(Am, Ac, Ap, lft, rgt, miss);                                          \
+      const float2 rv = f2((q >= 0 && q < ny) ? 1.f : 0.f);                                   \
+      Vn.a = mul2(mul2(fma2(CB, Bc.a, fma2(CA, Ac.a, mul2(CS, w.a))), xval.a), rv);           \
+      Vn.b = mul2(mul2(fma2(CB, Bc.b, fma2(CA, Ac.b, mul2(CS, w.b))), xval.b), rv);           \
+      if (io && q >= r0 && q < r1) f4_store(pJ + q * P, Vn);                                  \
+    }                                                                                         \
+    {                                                                                         \
+      const int r = q - 1;                                                                    \
+      const float lft = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                             \
+      if (r >= r0 && r < r1) {                                                                \
+        const float2 rm = f2(float((r == 0) + (r == ny - 1)));                                \
+        const F4 miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                             \
+        F4 z = lap4(Vm, Vc, Vn, lft, rgt, miss);                                              \
+        z.a = mul2(mul2(z.a, OP), xval.a);                                                    \
+        z.b = mul2(mul2(z.b, OP), xval.b);                                                    \
+        const F4 vm = F4{mul2(Am.a, SA), mul2(Am.b, SA)};                                     \
+        q0 = fma2(z.a, vm.a, fma2(z.b, vm.b, q0));                                            \
+        q1 = fma2(z.a, Vc.a, fma2(z.b, Vc.b, q1));                                            \
+        q2 = fma2(vm.a, Vc.a, fma2(vm.b, Vc.b, q2));                                          \
+        q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                              \
+        q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
+        q5 = fma2(vm.a, vm.a, fma2(vm.b, vm.b, q5));                                          \
+        if (++npair == 2) {                                                                   \
+          k0.add(q0.x + q0.y); k1.add(q1.x + q1.y); k2.add(q2.x + q2.y);                      \
+          k3.add(q3.x + q3.y); k4.add(q4.x + q4.y); k5.add(q5.x + q5.y);                      \
+          q0 = q1 = q2 = q3 = q4 = q5 = f2(0.f);                                              \
+          npair = 0;                                                                          \
+        }                                                                                     \
+      }                                                                                       \
+    }                                                                                         \
+    Af = rowA(q + 5);                                                                         \
+    Bc = rowB(q + 3);                                                                         \
+  }
+
+  for (int it0 = 0; it0 < nit; it0 += 6) {
+    int it = it0;
+    NLSB_ROW(A0, A1, A2, A0, B0, V1, V2, V0) ++it;
+    NLSB_ROW(A1, A2, A3, A1, B1, V2, V0, V1) ++it;
+    NLSB_ROW(A2, A3, A4, A2, B2, V0, V1, V2) ++it;
+    NLSB_ROW(A3, A4, A5, A3, B0, V1, V2, V0) ++it;
+    NLSB_ROW(A4, A5, A0, A4, B1, V2, V0, V1) ++it;
+    NLSB_ROW(A5, A0, A1, A5, B2, V0, V1, V2)
+  }
+#undef NLSB_ROW
+  k0.add(q0.x + q0.y); k1.add(q1.x + q1.y); k2.add(q2.x + q2.y);
+  k3.add(q3.x + q3.y); k4.add(q4.x + q4.y); k5.add(q5.x + q5.y);
+  constexpr int ND = 6;
+  double vals[ND] = {k0.val(), k1.val(), k2.val(), k3.val(), k4.val(), k5.val()};
+#pragma unroll
+  for (int q = 0; q < ND; ++q) vals[q] = io ? vals[q] : 0.0;
+  const int tc = s.tile_count, TT = *a.lt_stride;
+  if (warp_publish<ND>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot * 2 + sq,
+                       tc, lane)) {
+    const double *part = a.part + (long long)j * a.part_stride;
+    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin, tc, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
+      a.ticket[t.slot * 2 + sq] = 0;
+    }
+  }
+}
