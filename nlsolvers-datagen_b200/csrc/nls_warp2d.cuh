@@ -1136,21 +1136,6 @@ __global__ void __launch_bounds__(32 * WPB, 4) k2_lanczos1(StepArgs a) {
   }
 }
 
-// Bulk prefetch of a contiguous byte range into L2 (no registers, no
-// completion tracking): start 16-byte aligned, size a multiple of 16.
-__device__ __forceinline__ void l2_prefetch(const void *p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// Lane 0 prefetches row r of a strip of one field (elements [xb, xe) of the
-// row) into L2 when the row exists.
-template <typename E>
-__device__ __forceinline__ void strip_prefetch(const E *base, const SlotDesc &s, int xb, int xe, int r,
-                                               int lane) {
-  if (lane == 0 && r >= 0 && r < s.ny && xe > xb)
-    l2_prefetch(base + s.off + (long long)r * s.pitch + xb, (unsigned)((xe - xb) * sizeof(E)));
-}
-
 // -------------------------- FP32 Lanczos pass with packed FP32x2 arithmetic
 // The headline path (real FP32 fields, c == 1). Each lane's 16-byte vector is
 // two float2 pairs processed with the sm_100 packed FFMA2 / FADD2 / FMUL2
@@ -1255,17 +1240,6 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32(StepArgs a) {
   F4 B0 = rowB(r0 - 1), B1 = rowB(r0), B2 = rowB(r0 + 1);
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
   F4 V0 = zero4, V1 = zero4, V2 = zero4;
-  // the strip's element range incl. halo vectors, for the L2 prefetches
-  const int HLn = HaloLanes<4>::HL;
-  const int pxb = max(t.x0 - 4 * HLn, 0), pxe = min(t.x0 + 4 * (t.y0 + HLn), (int)s.pitch);
-  const float *gA = (const float *)a.V + (vo + j - 1) * a.vstride;
-  const float *gB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride;
-  constexpr int PF = 12;  // rows of L2 prefetch ahead of the register ring
-#pragma unroll 1
-  for (int d = 4; d < PF; ++d) {
-    strip_prefetch(gA, s, pxb, pxe, r0 + d, lane);
-    if (hasB) strip_prefetch(gB, s, pxb, pxe, r0 + d - 1, lane);
-  }
   const int qb = r0 - 1, qe = r1;  // v_j rows
   const int nit = ((qe - qb + 1) + 5) / 6 * 6;
 
@@ -1313,8 +1287,6 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32(StepArgs a) {
     }                                                                                         \
     Af = rowA(q + 5);                                                                         \
     Bc = rowB(q + 3);                                                                         \
-    strip_prefetch(gA, s, pxb, pxe, q + 1 + PF, lane);                                        \
-    if (hasB) strip_prefetch(gB, s, pxb, pxe, q + PF, lane);                                  \
   }
 
   for (int it0 = 0; it0 < nit; it0 += 6) {
