@@ -112,6 +112,21 @@ cudaError_t launch2_lanczos1_f32(const StepArgs &a, int tiles, cudaStream_t st) 
     k2_lanczos1_f32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
+cudaError_t launch2t_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2t_lanczos_f32<<<tiles, 128, sizeof(TmaSmem), st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t attrs_tma_f32() {
+  return set_smem(k2t_lanczos_f32, sizeof(TmaSmem));
+}
+// NLS_TMA=0 selects the register-ring FP32 pass instead of the TMA pipeline.
+bool use_tma() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_TMA");
+    return (e && std::atoi(e) == 0) ? 0 : 1;
+  }();
+  return v != 0;
+}
 template <typename E, int NSEQ, int FIN, bool HC>
 cudaError_t launch2_final(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_final<E, NSEQ, FIN, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
@@ -161,6 +176,7 @@ cudaError_t launch_advance(const StepArgs &a, int nslots_cap, cudaStream_t st) {
 struct KSet {
   Launch kg, ss2, sewi_a, sewi_b;  // Gautschi / NLSE phases
   LaunchFn sv[2] = {nullptr, nullptr};
+  LaunchFn lanczos_tma = nullptr;  // 2-D FP32 c == 1 TMA-pipelined pass (tile table `tt`)
   cudaError_t (*ftri)(const StepArgs &, int, cudaStream_t) = nullptr;
   cudaError_t (*ring)(const StepArgs &, int, int, cudaStream_t) = nullptr;
   cudaError_t (*set_attrs)() = nullptr;
@@ -223,14 +239,18 @@ template <typename R> KSet make_real2() {
   k.kg.first[1] = launch2_first<R, SRC_KG, true>;
   k.kg.lanczos[0] = launch2_lanczos1<R, false>;
   k.kg.lanczos[1] = launch2_lanczos1<R, true>;
-  if constexpr (sizeof(R) == 4) k.kg.lanczos[0] = launch2_lanczos1_f32;  // packed FP32x2 path
+  if constexpr (sizeof(R) == 4) {
+    k.kg.lanczos[0] = launch2_lanczos1_f32;  // packed FP32x2 path
+    k.lanczos_tma = launch2t_lanczos_f32;
+    k.set_attrs = attrs_tma_f32;
+  }
   k.kg.final_[0] = launch2_final<R, 2, FIN_KG, false>;
   k.kg.final_[1] = launch2_final<R, 2, FIN_KG, true>;
   k.sv[0] = launch2_sv<R, false>;
   k.sv[1] = launch2_sv<R, true>;
   k.ftri = launch_ftri<R>;
   k.ring = launch_ring<R, 0>;
-  k.set_attrs = attrs_none;
+  if (!k.set_attrs) k.set_attrs = attrs_none;
   return k;
 }
 template <typename E> KSet make_cplx2() {
@@ -343,6 +363,11 @@ struct TileSet {
   int lcap = 0;
   int lt_count2 = 0;  // host copy of 2 * live (source of the async upload)
   std::vector<TileDesc> lt;
+  // 2-D TMA passes: tiles of <= 512 columns x segment rows, one section per sequence
+  TileDesc *d_tt = nullptr;
+  int *d_ntt1 = nullptr, *d_ntt2 = nullptr;
+  int tcap = 0, tt_live = 0, tt_count2 = 0;
+  std::vector<TileDesc> tt;
 };
 
 }  // namespace
@@ -367,6 +392,7 @@ struct nls_pool {
   double *d_beta0 = nullptr;
   FinalCoef *d_coef = nullptr;
   int *d_ticket = nullptr;
+  void *zeros = nullptr;  // 32 KiB of zeros (source of out-of-grid rows)
   TileSet main, first;  // main step / SEWI Strang first steps
   std::vector<SlotHost> hs;
   std::vector<SlotDesc> sd;
@@ -378,7 +404,7 @@ struct nls_pool {
   cudaGraphExec_t gexec = nullptr;
   int graph_tiles = -1, graph_ring = -1, graph_hc = -1;
   void *graph_part = nullptr;
-  int graph_lcap = -1;
+  int graph_lcap = -1, graph_tcap = -1;
   int step_hc = 0;  // some stepped slot carries a c field
   int ring_blocks = 1;
   int kernels_per_step = 0;
@@ -423,7 +449,9 @@ void pool_free_device(nls_pool *P) {
                   P->d_beta0, P->d_coef, P->d_ticket, P->main.d_tiles, P->main.d_ntiles, P->main.d_list,
                   P->main.d_nlist, P->first.d_tiles, P->first.d_ntiles, P->first.d_list,
                   P->first.d_nlist, P->main.d_lt, P->main.d_nlt1, P->main.d_nlt2,
-                  P->first.d_lt, P->first.d_nlt1, P->first.d_nlt2};
+                  P->first.d_lt, P->first.d_nlt1, P->first.d_nlt2, P->main.d_tt,
+                  P->main.d_ntt1, P->main.d_ntt2, P->first.d_tt, P->first.d_ntt1,
+                  P->first.d_ntt2, P->zeros};
   for (void *b : bufs)
     if (b) cudaFree(b);
 }
@@ -544,12 +572,52 @@ int rebuild_tables(nls_pool *P) {
     if (T->live) CK(cudaMemcpyAsync(T->d_lt, T->lt.data(), sizeof(TileDesc) * n2, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlt1, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlt2, &T->lt_count2, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+    if (P->dim == 2) {
+      std::vector<TileDesc> base;
+      for (int sidx : T->list) {
+        SlotDesc &d = P->sd[sidx];
+        d.tile_begin2 = (int)base.size();
+        const int nx4 = (d.nx + 3) / 4 * 4;
+        int local = 0;
+        for (int p0 = 0; p0 < d.ny; p0 += P->seg2)
+          for (int x0 = 0; x0 < nx4; x0 += 512) {
+            TileDesc tq;
+            tq.slot = sidx;
+            tq.x0 = x0;
+            tq.y0 = std::min(512, nx4 - x0);
+            tq.p0 = p0;
+            tq.p1 = std::min(d.ny, p0 + P->seg2);
+            tq.local = 2 * local++;
+            base.push_back(tq);
+          }
+        d.tile_count2 = local;
+      }
+      T->tt_live = (int)base.size();
+      T->tt.clear();
+      for (int sq = 0; sq < 2; ++sq)
+        for (TileDesc tq : base) {
+          tq.local += sq;
+          T->tt.push_back(tq);
+        }
+      T->tt_count2 = (int)T->tt.size();
+      if (T->tt_count2 > T->tcap || !T->d_tt) {
+        if (T->d_tt) cudaFree(T->d_tt);
+        T->d_tt = nullptr;
+        T->tcap = std::max(T->tt_count2, 128);
+        CK(cudaMalloc(&T->d_tt, sizeof(TileDesc) * T->tcap));
+      }
+      if (T->tt_count2)
+        CK(cudaMemcpyAsync(T->d_tt, T->tt.data(), sizeof(TileDesc) * T->tt_count2, cudaMemcpyHostToDevice, P->stream));
+      CK(cudaMemcpyAsync(T->d_ntt1, &T->tt_live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+      CK(cudaMemcpyAsync(T->d_ntt2, &T->tt_count2, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+    }
     if (T->live) CK(cudaMemcpyAsync(T->d_tiles, T->tiles.data(), sizeof(TileDesc) * T->live, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_ntiles, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     if (T->nlist) CK(cudaMemcpyAsync(T->d_list, T->list.data(), sizeof(int) * T->nlist, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlist, &T->nlist, sizeof(int), cudaMemcpyHostToDevice, P->stream));
   }
-  int rc = ensure_partials(P, std::max(P->main.lcap, P->first.lcap));
+  int rc = ensure_partials(P, std::max(std::max(P->main.lcap, P->first.lcap),
+                                       std::max(P->main.tcap, P->first.tcap)));
   if (rc) return rc;
   CK(cudaMemcpyAsync(P->d_slots, P->sd.data(), sizeof(SlotDesc) * P->max_slots, cudaMemcpyHostToDevice, P->stream));
   // the pageable sources above are staged by the runtime before returning;
@@ -588,6 +656,7 @@ StepArgs base_args(const nls_pool *P, const TileSet &T) {
   a.beta0 = P->d_beta0;
   a.coef = P->d_coef;
   a.ticket = P->d_ticket;
+  a.zeros = P->zeros;
   a.scal_ready = P->dim == 2 ? 1 : 0;
   a.has_c = P->step_hc;
   return a;
@@ -598,9 +667,16 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
   const int grid = T.cap, hc = P->step_hc;
   CK(L.first[hc](a, grid, P->stream));
   ++nk;
-  StepArgs b = a;  // 2-D passes: one warp per (strip, sequence)
+  StepArgs b = a;  // 2-D passes: one warp per (strip, sequence) or one TMA block per tile
   int lgrid = grid;
-  if (P->dim == 2) {
+  LaunchFn lf = L.lanczos[hc];
+  if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
+    b.tiles = T.d_tt;
+    b.ntiles = a.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
+    b.lt_stride = T.d_ntt1;
+    lgrid = T.tcap;
+    lf = P->ks.lanczos_tma;
+  } else if (P->dim == 2) {
     b.tiles = T.d_lt;
     b.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
     b.lt_stride = T.d_nlt1;
@@ -608,7 +684,7 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
   }
   for (int j = 1; j <= P->k - 2; ++j) {
     b.j = j;
-    CK(L.lanczos[hc](b, lgrid, P->stream));
+    CK(lf(b, lgrid, P->stream));
     ++nk;
   }
   CK(P->ks.ftri(a, P->max_slots, P->stream));
@@ -682,7 +758,7 @@ int run_main_step(nls_pool *P) {
   if (!P->use_graph) return enqueue_step(P, P->main, false);
   if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks ||
       P->graph_hc != P->step_hc || P->graph_part != (void *)P->part ||
-      P->graph_lcap != P->main.lcap) {
+      P->graph_lcap != P->main.lcap || P->graph_tcap != P->main.tcap) {
     if (P->gexec) {
       cudaGraphExecDestroy(P->gexec);
       P->gexec = nullptr;
@@ -704,6 +780,7 @@ int run_main_step(nls_pool *P) {
     P->graph_hc = P->step_hc;
     P->graph_part = (void *)P->part;
     P->graph_lcap = P->main.lcap;
+    P->graph_tcap = P->main.tcap;
   }
   CK(cudaGraphLaunch(P->gexec, P->stream));
   return NLS_OK;
@@ -970,7 +1047,10 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_beta0, sizeof(double) * max_slots * 2);
   if (!rc) rc = al((void **)&P->d_coef, sizeof(FinalCoef) * max_slots * 2);
   if (!rc) rc = al((void **)&P->d_ticket, sizeof(int) * max_slots * 2);
+  if (!rc) rc = al(&P->zeros, 32768);
   for (TileSet *T : {&P->main, &P->first}) {
+    if (!rc) rc = al((void **)&T->d_ntt1, sizeof(int));
+    if (!rc) rc = al((void **)&T->d_ntt2, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlt1, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlt2, sizeof(int));
     if (!rc) rc = al((void **)&T->d_ntiles, sizeof(int));
@@ -989,6 +1069,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
     if (e == cudaSuccess) e = cudaMemsetAsync(P->snap, 0, sizeof(double) * ce * 2 * NF, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->d_coef, 0, sizeof(FinalCoef) * max_slots * 2, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->d_ticket, 0, sizeof(int) * max_slots * 2, P->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->zeros, 0, 32768, P->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
     if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -1236,15 +1317,22 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
   CK(cudaEventCreate(&e1));
   const int hc = P->step_hc;
   int grid = P->main.cap;
-  if (P->dim == 2) {
+  LaunchFn lf = L.lanczos[hc];
+  if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
+    a.tiles = P->main.d_tt;
+    a.ntiles = a.nseq == 2 ? P->main.d_ntt2 : P->main.d_ntt1;
+    a.lt_stride = P->main.d_ntt1;
+    grid = P->main.tcap;
+    lf = P->ks.lanczos_tma;
+  } else if (P->dim == 2) {
     a.tiles = P->main.d_lt;
     a.ntiles = a.nseq == 2 ? P->main.d_nlt2 : P->main.d_nlt1;
     a.lt_stride = P->main.d_nlt1;
     grid = P->main.lcap;
   }
-  CK(L.lanczos[hc](a, grid, P->stream));  // warm
+  CK(lf(a, grid, P->stream));  // warm
   CK(cudaEventRecord(e0, P->stream));
-  for (int i = 0; i < iters; ++i) CK(L.lanczos[hc](a, grid, P->stream));
+  for (int i = 0; i < iters; ++i) CK(lf(a, grid, P->stream));
   CK(cudaEventRecord(e1, P->stream));
   CK(cudaEventSynchronize(e1));
   float t = 0.f;

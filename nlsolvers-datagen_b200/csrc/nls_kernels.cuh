@@ -63,6 +63,7 @@ struct StepArgs {
   int sv_pingpong;       // SV step: u_hi / u_alt alternate by step parity
   int *ticket;           // [slot][seq] arrival counters of the 2-D passes
   const int *lt_stride;  // device scalar: tiles per sequence section of the 2-D pass table
+  const void *zeros;     // device buffer of zeros (source of out-of-grid rows)
   int scal_ready;        // 1: every pass published its scalars (2-D path)
 };
 

@@ -23,6 +23,7 @@ struct SlotDesc {
   int64_t n;                 // nx*ny*nz (unpadded points)
   int32_t active;
   int32_t variant;           // NLSE SEWI operand order: 0 reference, 1 corrected
+  int32_t tile_begin2, tile_count2;  // tiles of the TMA-pipelined 2-D passes
 };
 
 // Mutable per-slot state on the device (advanced by the boundary kernel).
