@@ -119,11 +119,12 @@ cudaError_t launch2t_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) 
 cudaError_t attrs_tma_f32() {
   return set_smem(k2t_lanczos_f32, sizeof(TmaSmem));
 }
-// NLS_TMA=0 selects the register-ring FP32 pass instead of the TMA pipeline.
+// NLS_TMA=1 selects the TMA-pipelined FP32 pass; the register-ring pass is the
+// default (it issues half the instructions and needs no per-row barrier).
 bool use_tma() {
   static int v = [] {
     const char *e = std::getenv("NLS_TMA");
-    return (e && std::atoi(e) == 0) ? 0 : 1;
+    return (e && std::atoi(e) == 1) ? 1 : 0;
   }();
   return v != 0;
 }
