@@ -147,6 +147,32 @@ int nls_host_free(void *ptr);
    (one process per GPU; the library keeps its own runtime state). */
 int nls_set_device(int32_t device);
 
+/* ---- no-allocation Gautschi step. No counterpart in the reference: its
+   MatrixFunctionApplicatorReal::apply allocates device memory on every call
+   (matfunc_real.hpp:190-313). For callers that cannot allocate device memory
+   (a solver embedded in a code that owns and caps the memory pool) this
+   advances the reference's own device state in place: u (n doubles) and
+   u_past (n doubles, KGESolverDevice's d_u / d_u_past, kg_dev.hpp:32-131),
+   with m (and c, NULL when c == 1), all device pointers, C order (ny, nx).
+   Method NLS_KG_GAUTSCHI or NLS_SP4_GAUTSCHI, dim 2, FP32 or FP64 arithmetic.
+   Each step is the pool step (Krylov matrix functions, update, ghost copies);
+   first_step is the driver-loop index i of the first step (keys the phi^4
+   noise). All working memory is one static device array of
+   NLS_NOALLOC_SCRATCH_BYTES per device; a grid that needs more (about
+   (20 + 8(k-1)) bytes per padded point in FP32, twice that in FP64) is
+   rejected with NLS_ERR_CAPACITY, whose message gives both sizes. The call
+   allocates nothing, issues no host-to-device copy and returns after the
+   steps completed on `stream` (a cudaStream_t; NULL: the legacy stream).
+   The first call on a device does the set-up (loads the kernels and looks up
+   the scratch address); make it before any stream capture. Every call
+   re-initialises what must start at zero (reduction tickets, step state), so
+   nothing needs clearing between calls. All calls on one device share the
+   scratch: calls that overlap in time (from several threads or streams) race
+   and must be serialised by the caller. */
+#define NLS_NOALLOC_SCRATCH_BYTES (32u << 20)
+int nls_gautschi_step_noalloc(const nls_problem *p, double *u, double *u_past, const double *m,
+                              const double *c, int32_t first_step, int32_t nsteps, void *stream);
+
 const char *nls_strerror(int code);
 /* Copy the calling thread's last error message (NUL-terminated). */
 int nls_last_error(char *buf, int32_t len);

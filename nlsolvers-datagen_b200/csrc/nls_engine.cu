@@ -30,6 +30,15 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+}  // namespace
+
+// Error reporting shared with the other translation units of the library.
+namespace nlsb {
+int api_fail(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace nlsb
+
+namespace {
+
 #define CK(call)                                                                     \
   do {                                                                               \
     cudaError_t e_ = (call);                                                         \

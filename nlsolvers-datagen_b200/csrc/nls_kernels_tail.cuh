@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(256) k_ring(StepArgs a) {
   }
 }
 
-__global__ void k_advance(StepArgs a) {
+static __global__ void k_advance(StepArgs a) {
   const int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= *a.nslot_list) return;
   a.state[a.slot_list[li]].step += 1;

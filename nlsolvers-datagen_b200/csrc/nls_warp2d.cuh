@@ -1386,7 +1386,7 @@ struct TmaSmem {
   int last;
 };
 
-__global__ void __launch_bounds__(128, 3) k2t_lanczos_f32(StepArgs a) {
+static __global__ void __launch_bounds__(128, 3) k2t_lanczos_f32(StepArgs a) {
   extern __shared__ __align__(128) unsigned char tma_raw[];
   TmaSmem &M = *reinterpret_cast<TmaSmem *>(tma_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
