@@ -96,6 +96,10 @@ int nls_run(nls_handle *h);
 /* Copy the ns snapshots (ns*n values) to host: traj (NLSE: complex128), vel
    (KG/phi4 only, may be NULL). Waits for outstanding work. */
 int nls_snapshot(nls_handle *h, double *traj, double *vel);
+/* Per-snapshot diagnostics of a single trajectory (layout and meaning as
+   nls_pool_set_diagnostics); call before the first step; complete after
+   nls_snapshot. */
+int nls_set_diagnostics(nls_handle *h, double *diag_dst);
 /* Steps completed so far. */
 int nls_steps_done(nls_handle *h, int32_t *steps);
 int nls_destroy(nls_handle *h);
@@ -116,6 +120,19 @@ int nls_pool_step(nls_pool *pool, int32_t nsteps);
 /* steps_done: completed steps; finished: 1 when all steps ran and every
    snapshot has reached the host buffers. */
 int nls_pool_poll(nls_pool *pool, int32_t slot, int32_t *steps_done, int32_t *finished);
+/* Per-snapshot energy and mass (the reference computes them post hoc from the
+   snapshots: scripts/compare_utils_real_2d.py:112-131,
+   scripts/compare_utils_complex_2d.py:134-151). Call once, after admission and
+   before the slot's first step; diag_dst (ns x 4 doubles, kept valid until
+   release) receives, for each snapshot s, with central differences on the
+   interior and dA = dx dy (dx dy dz in 3-D, dz = 2 Lz/(nz-1)):
+     KG / phi4: [s*4 + 0..3] = 1/2 sum v^2 dA, 1/2 sum c |grad u|^2 dA,
+                                sum m u^4/4 dA, sum u^2 dA
+     NLSE:      [s*4 + 0..3] = sum |u|^2 dA, sum |grad u|^2 dA,
+                                -1/2 sum |u|^4 dA, 0
+   computed on the device from the FP64 snapshot (m, c as stored: FP32 in an
+   FP32 pool) and copied with the snapshot; complete when the snapshot is. */
+int nls_pool_set_diagnostics(nls_pool *pool, int32_t slot, double *diag_dst);
 /* Free the slot (waits for its outstanding snapshot copies). */
 int nls_pool_release(nls_pool *pool, int32_t slot);
 /* Wait for all queued device work and copies. */

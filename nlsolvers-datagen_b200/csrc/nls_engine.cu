@@ -357,6 +357,8 @@ struct SlotHost {
   bool copy_pending[NF] = {false, false};
   bool needs_ss2 = false;  // SEWI: first step is a Strang step
   int ring_cnt = 0;
+  double *diag = nullptr;  // ns x 4 diagnostics (host), or null
+  bool reg_diag = false;
 };
 
 struct TileSet {
@@ -403,6 +405,8 @@ struct nls_pool {
   FinalCoef *d_coef = nullptr;
   int *d_ticket = nullptr;
   void *zeros = nullptr;  // 32 KiB of zeros (source of out-of-grid rows)
+  double *d_diag_part = nullptr, *d_diag_out = nullptr;  // per slot: k_diag partials / result
+  int *d_diag_ticket = nullptr;
   TileSet main, first;  // main step / SEWI Strang first steps
   std::vector<SlotHost> hs;
   std::vector<SlotDesc> sd;
@@ -461,7 +465,7 @@ void pool_free_device(nls_pool *P) {
                   P->first.d_nlist, P->main.d_lt, P->main.d_nlt1, P->main.d_nlt2,
                   P->first.d_lt, P->first.d_nlt1, P->first.d_nlt2, P->main.d_tt,
                   P->main.d_ntt1, P->main.d_ntt2, P->first.d_tt, P->first.d_ntt1,
-                  P->first.d_ntt2, P->zeros};
+                  P->first.d_ntt2, P->zeros, P->d_diag_part, P->d_diag_out, P->d_diag_ticket};
   for (void *b : bufs)
     if (b) cudaFree(b);
 }
@@ -803,6 +807,33 @@ int wait_frame(nls_pool *P, SlotHost &h, int step) {
   return NLS_OK;
 }
 
+// Diagnostics of snapshot si of slot s from device frame f, then their D2H.
+int enqueue_diag(nls_pool *P, int s, int si, int f, cudaStream_t st) {
+  SlotHost &h = P->hs[s];
+  const SlotDesc &d = P->sd[s];
+  const double *frame = P->snap + d.snap_off + (int64_t)f * 2 * h.n;
+  const nls_problem &p = h.prob;
+  const double dx = 2 * p.Lx / (p.nx - 1), dy = 2 * p.Ly / (p.ny - 1);
+  const double dz = p.dim == 3 ? 2 * p.Lz / (p.nz - 1) : 1.0;
+  const int blocks = (int)std::min<int64_t>(DIAG_BLOCKS, (h.n + 1023) / 1024);
+  double *part = P->d_diag_part + (int64_t)s * DIAG_BLOCKS * 4, *out = P->d_diag_out + (int64_t)s * 4;
+  int *tk = P->d_diag_ticket + s;
+  if (P->prec == NLS_FP64) {
+    if (P->cplx)
+      k_diag<double, true><<<blocks, 256, 0, st>>>(frame, (const double *)P->m, (const double *)P->c, d, dx, dy, dz, part, tk, out);
+    else
+      k_diag<double, false><<<blocks, 256, 0, st>>>(frame, (const double *)P->m, (const double *)P->c, d, dx, dy, dz, part, tk, out);
+  } else {
+    if (P->cplx)
+      k_diag<float, true><<<blocks, 256, 0, st>>>(frame, (const float *)P->m, (const float *)P->c, d, dx, dy, dz, part, tk, out);
+    else
+      k_diag<float, false><<<blocks, 256, 0, st>>>(frame, (const float *)P->m, (const float *)P->c, d, dx, dy, dz, part, tk, out);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h.diag + (int64_t)si * 4, out, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+  return NLS_OK;
+}
+
 int issue_copies(nls_pool *P, SlotHost &h, const SlotDesc &d, int step) {
   if (step % h.freq != 0 || step / h.freq >= h.ns) return NLS_OK;
   const int si = step / h.freq, f = si % NF;
@@ -816,6 +847,10 @@ int issue_copies(nls_pool *P, SlotHost &h, const SlotDesc &d, int step) {
     if (h.vel)
       CK(cudaMemcpyAsync(h.vel + (int64_t)si * h.n, frame + h.n, sizeof(double) * h.n,
                          cudaMemcpyDeviceToHost, P->copy_stream));
+  }
+  if (h.diag) {
+    int rc = enqueue_diag(P, (int)(&h - P->hs.data()), si, f, P->copy_stream);
+    if (rc) return rc;
   }
   CK(cudaEventRecord(h.copy_done[f], P->copy_stream));
   h.copy_pending[f] = true;
@@ -1058,6 +1093,9 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_coef, sizeof(FinalCoef) * max_slots * 2);
   if (!rc) rc = al((void **)&P->d_ticket, sizeof(int) * max_slots * 2);
   if (!rc) rc = al(&P->zeros, 32768);
+  if (!rc) rc = al((void **)&P->d_diag_part, sizeof(double) * max_slots * DIAG_BLOCKS * 4);
+  if (!rc) rc = al((void **)&P->d_diag_out, sizeof(double) * max_slots * 4);
+  if (!rc) rc = al((void **)&P->d_diag_ticket, sizeof(int) * max_slots);
   for (TileSet *T : {&P->main, &P->first}) {
     if (!rc) rc = al((void **)&T->d_ntt1, sizeof(int));
     if (!rc) rc = al((void **)&T->d_ntt2, sizeof(int));
@@ -1080,6 +1118,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
     if (e == cudaSuccess) e = cudaMemsetAsync(P->d_coef, 0, sizeof(FinalCoef) * max_slots * 2, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->d_ticket, 0, sizeof(int) * max_slots * 2, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->zeros, 0, 32768, P->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->d_diag_ticket, 0, sizeof(int) * max_slots, P->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
     if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -1257,12 +1296,31 @@ int nls_pool_release(nls_pool *P, int32_t s) {
   CK(cudaStreamSynchronize(P->stream));
   if (h.reg_traj) cudaHostUnregister(h.traj);
   if (h.reg_vel) cudaHostUnregister(h.vel);
+  if (h.reg_diag) cudaHostUnregister(h.diag);
   P->arena.release(h.off, h.npad);
   P->snap_arena.release(h.snap_off, 2 * NF * h.n);
   h = SlotHost();
   P->sd[s].active = 0;
   P->tables_dirty = true;
   return NLS_OK;
+}
+
+int nls_pool_set_diagnostics(nls_pool *P, int32_t s, double *diag_dst) {
+  if (!P || !diag_dst) return fail(NLS_ERR_INVALID_ARG, "null argument");
+  if (s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
+  SlotHost &h = P->hs[s];
+  if (h.step != 1 || h.diag) return fail(NLS_ERR_STATE, "diagnostics must be enabled once, before the slot's first step");
+  h.diag = diag_dst;
+  h.reg_diag = cudaHostRegister(diag_dst, sizeof(double) * 4 * h.ns, cudaHostRegisterDefault) == cudaSuccess;
+  cudaGetLastError();  // a failed registration only makes the copies synchronous
+  std::memset(diag_dst, 0, sizeof(double) * 4 * h.ns);
+  // snapshot 0: the input state, written into frame 0 at admission
+  return enqueue_diag(P, s, 0, 0, P->stream);
+}
+
+int nls_set_diagnostics(nls_handle *H, double *diag_dst) {
+  if (!H) return fail(NLS_ERR_INVALID_ARG, "null handle");
+  return nls_pool_set_diagnostics(H->pool, H->slot, diag_dst);
 }
 
 int nls_pool_sync(nls_pool *P) {

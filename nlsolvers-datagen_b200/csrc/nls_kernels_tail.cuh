@@ -386,6 +386,100 @@ static __global__ void k_advance(StepArgs a) {
   a.state[a.slot_list[li]].step += 1;
 }
 
+// ------------------------------------------------------- diagnostics
+// Energy and mass of one FP64 snapshot frame, as the reference computes them
+// post hoc: KG (scripts/compare_utils_real_2d.py:112-131) out = {1/2 sum v^2 dA,
+// 1/2 sum_interior c (ux^2 + uy^2) dA, sum m u^4/4 dA, sum u^2 dA}; NLSE
+// (scripts/compare_utils_complex_2d.py:134-151) out = {sum |u|^2 dA,
+// sum_interior (|ux|^2 + |uy|^2) dA, -1/2 sum |u|^4 dA, 0}. Derivatives are
+// central differences on the interior points (all axes away from the ghost
+// ring); 3-D adds the z term and dA = dx dy dz. Per-thread FP64 sums, a fixed
+// shared-memory tree per block, and the last block (ticket) adds the block
+// partials in block order: the result does not depend on scheduling.
+constexpr int DIAG_BLOCKS = 64;
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(256) k_diag(const double *frame, const R *m, const R *c, SlotDesc s,
+                                              double dx, double dy, double dz, double *part, int *ticket,
+                                              double *out) {
+  __shared__ double red[4][256];
+  __shared__ bool last;
+  const int nx = s.nx, ny = s.ny, nz = s.dim == 3 ? s.nz : 1;
+  const long long n = (long long)nx * ny * nz, plane = (long long)nx * ny;
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  const double ix = 1.0 / (2.0 * dx), iy = 1.0 / (2.0 * dy), iz = 1.0 / (2.0 * dz);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(p % nx);
+    const int y = (int)((p / nx) % ny);
+    const int z = (int)(p / plane);
+    const bool inner = x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && (s.dim == 2 || (z > 0 && z < nz - 1));
+    const long long e = s.off + ((long long)z * ny + y) * s.pitch + x;
+    if (CPLX) {
+      const double ur = frame[2 * p], ui = frame[2 * p + 1], u2 = ur * ur + ui * ui;
+      a0 += u2;
+      a2 += u2 * u2;
+      if (inner) {
+        const double gxr = (frame[2 * (p + 1)] - frame[2 * (p - 1)]) * ix;
+        const double gxi = (frame[2 * (p + 1) + 1] - frame[2 * (p - 1) + 1]) * ix;
+        const double gyr = (frame[2 * (p + nx)] - frame[2 * (p - nx)]) * iy;
+        const double gyi = (frame[2 * (p + nx) + 1] - frame[2 * (p - nx) + 1]) * iy;
+        double g = gxr * gxr + gxi * gxi + gyr * gyr + gyi * gyi;
+        if (s.dim == 3) {
+          const double gzr = (frame[2 * (p + plane)] - frame[2 * (p - plane)]) * iz;
+          const double gzi = (frame[2 * (p + plane) + 1] - frame[2 * (p - plane) + 1]) * iz;
+          g += gzr * gzr + gzi * gzi;
+        }
+        a1 += g;
+      }
+    } else {
+      const double u = frame[p], v = frame[n + p], u2 = u * u;
+      a0 += v * v;
+      a2 += (double)m[e] * (0.25 * u2 * u2);
+      a3 += u2;
+      if (inner) {
+        const double gx = (frame[p + 1] - frame[p - 1]) * ix;
+        const double gy = (frame[p + nx] - frame[p - nx]) * iy;
+        double g = gx * gx + gy * gy;
+        if (s.dim == 3) {
+          const double gz = (frame[p + plane] - frame[p - plane]) * iz;
+          g += gz * gz;
+        }
+        a1 += (double)c[e] * g;
+      }
+    }
+  }
+  red[0][threadIdx.x] = a0;
+  red[1][threadIdx.x] = a1;
+  red[2][threadIdx.x] = a2;
+  red[3][threadIdx.x] = a3;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 4) {
+    double t = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) t += ((volatile double *)part)[b * 4 + threadIdx.x];
+    const double dA = dx * dy * (s.dim == 3 ? dz : 1.0);
+    double r;
+    if (CPLX) {
+      r = threadIdx.x == 0 ? t * dA : threadIdx.x == 1 ? t * dA : threadIdx.x == 2 ? -0.5 * t * dA : 0.0;
+    } else {
+      r = threadIdx.x == 0 ? 0.5 * t * dA : threadIdx.x == 1 ? 0.5 * t * dA : t * dA;
+    }
+    out[threadIdx.x] = r;
+  }
+  if (threadIdx.x == 0) *ticket = 0;
+}
+
 // Admission: FP64 host inputs (staged on the device) -> the slot's padded
 // layout. hi = (R)u, lo = (R)(u - hi) (exactly representable remainder), the
 // KG increment d = u0 - (u0 - dt v0) as kg_dev.hpp:55-58 forms u_past, c = 1
@@ -426,6 +520,17 @@ __global__ void k_admit(StepArgs a, int slot, const double *u0, const double *v0
       const double v = (in && has_v) ? v0[pt] : 0.0;
       const double up = u - s.dt * v;
       ((R *)a.f.d)[g] = (R)(u - up);
+    }
+    // snapshot 0 (the input, exact) in frame 0: the source of its diagnostics
+    if (in) {
+      double *F0 = a.f.snap + s.snap_off;
+      if (NC == 2) {
+        F0[2 * pt] = u0[2 * pt];
+        F0[2 * pt + 1] = u0[2 * pt + 1];
+      } else {
+        F0[pt] = u0[pt];
+        F0[s.n + pt] = has_v ? v0[pt] : 0.0;
+      }
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -32,7 +32,7 @@ SYMBOLS = [
     "nls_pool_set_graphs", "nls_pool_set_segment", "nls_pool_time_pass",
     "nls_pool_kernels_per_step", "nls_pool_destroy", "nls_strerror", "nls_last_error",
     "nls_pool_step_timed", "nls_set_device", "nls_host_alloc", "nls_host_free",
-    "nls_gautschi_step_noalloc",
+    "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
 ]
 
 
@@ -105,6 +105,8 @@ def lib() -> ctypes.CDLL:
         "nls_host_free": [vp],
         "nls_last_error": [ctypes.c_char_p, i32],
         "nls_gautschi_step_noalloc": [pp, vp, vp, vp, vp, i32, i32, vp],
+        "nls_pool_set_diagnostics": [vp, i32, dp],
+        "nls_set_diagnostics": [vp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -144,6 +144,18 @@ class Solver:
     def run(self):
         check(lib().nls_run(self._h))
 
+    def enable_diagnostics(self):
+        """Per-snapshot energy / mass (ns x 4, filled as snapshots complete;
+        see nls_pool_set_diagnostics). Call before the first step."""
+        self._diag = np.zeros((self.spec.ns, 4))
+        check(lib().nls_set_diagnostics(self._h, _dptr(self._diag)))
+        return self._diag
+
+    def diagnostics(self):
+        """The diagnostics array after waiting for all snapshots."""
+        self.snapshots()
+        return self._diag
+
     def steps_done(self) -> int:
         v = ctypes.c_int32()
         check(lib().nls_steps_done(self._h, ctypes.byref(v)))
@@ -181,6 +193,7 @@ class SlotInfo:
     traj: np.ndarray
     vel: np.ndarray | None
     inputs: tuple = field(default_factory=tuple)
+    diag: np.ndarray | None = None
 
 
 class Pool:
@@ -221,6 +234,14 @@ class Pool:
         check(rc)
         self.slots[slot.value] = SlotInfo(slot.value, spec, traj, vel, (u0, v0, m, c))
         return slot.value
+
+    def enable_diagnostics(self, slot: int):
+        """Per-snapshot energy / mass of `slot` (ns x 4; see
+        nls_pool_set_diagnostics); call before the slot's first step."""
+        info = self.slots[slot]
+        info.diag = np.zeros((info.spec.ns, 4))
+        check(lib().nls_pool_set_diagnostics(self._p, slot, _dptr(info.diag)))
+        return info.diag
 
     def step(self, nsteps: int = 1):
         check(lib().nls_pool_step(self._p, int(nsteps)))

@@ -197,3 +197,18 @@ def test_nlse_ss2_mass_conserved(oracle_mod):
     traj, _ = run(p, u0, None, np.ones((n, n)), np.ones((n, n)))
     mass = (np.abs(traj) ** 2).sum(axis=(1, 2))
     assert np.abs(mass / mass[0] - 1).max() < 2e-3  # ghost copies change the mass slightly
+
+
+def test_diagnostics_restatement_matches_reference_functions():
+    """The oracle's diagnostics against the golden outputs of the reference's
+    own compute_hamiltonian_* / compute_mass* (tests/golden/diagnostics.npz)."""
+    import os
+    from oracle import diagnostics as D
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "diagnostics.npz"))
+    for i in range(2):
+        nx, ny, Lx, Ly = g[f"kg{i}_geom"]
+        got = D.kg(g[f"kg{i}_u"], g[f"kg{i}_v"], g[f"kg{i}_m"], g[f"kg{i}_c"], (Ly, Lx))
+        np.testing.assert_allclose(got, g[f"kg{i}_diag"], rtol=1e-13, atol=0)
+        nx, ny, Lx, Ly = g[f"nlse{i}_geom"]
+        got = D.nlse(g[f"nlse{i}_u"], (Ly, Lx))
+        np.testing.assert_allclose(got, g[f"nlse{i}_diag"], rtol=1e-13, atol=1e-300)
