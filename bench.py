@@ -232,14 +232,15 @@ def run_small(args, lrank):
     B, k = args.batch, 10
     cases = make_batch(B, 0, k)
     cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
-    pool = Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=32)
+    pool = Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg)
     for cs in cases:
         assert pool.admit(*cs) is not None
     pool.step(args.warmup)
     ms = pool.step_timed(args.steps)
     pool.sync()
-    print(json.dumps({"small": True, "batch": B, "k": k, "ms_per_step": ms / args.steps,
-                      "kernels_per_step": pool.kernels_per_step()}), flush=True)
+    pass_ms, _ = pool.time_pass(2, 20)
+    print(json.dumps({"small": True, "batch": B, "k": k, "seg": args.seg, "ms_per_step": ms / args.steps,
+                      "pass_ms": pass_ms, "kernels_per_step": pool.kernels_per_step()}), flush=True)
     pool.close()
     return 0
 
@@ -374,6 +375,7 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
+    ap.add_argument("--seg", type=int, default=32, help="segment rows of the --small case")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -121,6 +121,22 @@ cudaError_t launch2_lanczos1_f32(const StepArgs &a, int tiles, cudaStream_t st) 
     k2_lanczos1_f32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
+// Packed FP32 pass form: 2 (default) interior fast path + FP64 dot flushes,
+// 1 the first form (per-row Kahan, row masks everywhere); NLS_F32_PASS selects.
+int f32_pass_form() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_F32_PASS");
+    return (e && std::atoi(e) == 1) ? 1 : 2;
+  }();
+  return v;
+}
+cudaError_t launch2_lanczos1_f32b(const StepArgs &a, int tiles, cudaStream_t st) {
+  if (f32_minb() == 3)
+    k2_lanczos1_f32b<3><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  else
+    k2_lanczos1_f32b<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
 cudaError_t launch2t_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   k2t_lanczos_f32<<<tiles, 128, sizeof(TmaSmem), st>>>(a);
   return cudaGetLastError();
@@ -250,7 +266,7 @@ template <typename R> KSet make_real2() {
   k.kg.lanczos[0] = launch2_lanczos1<R, false>;
   k.kg.lanczos[1] = launch2_lanczos1<R, true>;
   if constexpr (sizeof(R) == 4) {
-    k.kg.lanczos[0] = launch2_lanczos1_f32;  // packed FP32x2 path
+    k.kg.lanczos[0] = f32_pass_form() == 1 ? launch2_lanczos1_f32 : launch2_lanczos1_f32b;  // packed FP32x2
     k.lanczos_tma = launch2t_lanczos_f32;
     k.set_attrs = attrs_tma_f32;
   }

@@ -1320,6 +1320,164 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32(StepArgs a) {
   }
 }
 
+// Second form of the packed FP32 pass, with less work per row:
+//  - segments whose rows r0-2 .. r1+1 are interior rows of the grid (r0 >= 2,
+//    r1 <= ny-2) run a march without row predicates or row masks (EDGE false);
+//    the first and last segment of each trajectory keep them (EDGE true);
+//  - the column mask of v_j and z is folded into the per-lane coefficients
+//    (V rows outside the grid columns are zero, so only the stencil term needs it);
+//  - dot products: FP32 pair sums over three rows, added into FP64 accumulators;
+//    the scale of V_{j-1} (1/beta0 at j = 1) is applied to the finished sums;
+//  - rows are prefetched only up to the last row the segment needs.
+template <bool EDGE>
+__device__ __forceinline__ void lz1f32_march(const float *pA, const float *pB, float *pJ, int P, int r0, int r1,
+                                             int ny, bool ld, bool io, bool hasB, float2 CA, float2 CB,
+                                             const F4 &CSx, const F4 &OPx, const F4 &xmiss, double *acc) {
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  auto rowA = [&](int r) -> F4 {
+    const bool ok = EDGE ? (ld && r >= 0 && r < ny && r <= r1 + 1) : (ld && r <= r1 + 1);
+    return ok ? f4_load(pA + r * P) : zero4;
+  };
+  auto rowB = [&](int r) -> F4 {
+    const bool ok = EDGE ? (ld && hasB && r >= 0 && r < ny && r <= r1) : (ld && hasB && r <= r1);
+    return ok ? f4_load(pB + r * P) : zero4;
+  };
+  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f), q5 = f2(0.f);
+  F4 A0 = rowA(r0 - 2), A1 = rowA(r0 - 1), A2 = rowA(r0), A3 = rowA(r0 + 1), A4 = rowA(r0 + 2),
+     A5 = rowA(r0 + 3);
+  F4 B0 = rowB(r0 - 1), B1 = rowB(r0), B2 = rowB(r0 + 1);
+  F4 V0 = zero4, V1 = zero4, V2 = zero4;
+  const int qb = r0 - 1;
+  const int nit = ((r1 - qb + 1) + 5) / 6 * 6;
+#define NLSB_ROW2(Am, Ac, Ap, Af, Bc, Vm, Vc, Vn, FLUSH)                                        \
+  {                                                                                           \
+    const int q = qb + it;                                                                    \
+    {                                                                                         \
+      const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
+      F4 miss = xmiss;                                                                        \
+      if (EDGE) {                                                                             \
+        const float2 rm = f2(float((q == 0) + (q == ny - 1)));                                \
+        miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                      \
+      }                                                                                       \
+      const F4 w = lap4(Am, Ac, Ap, lft, rgt, miss);                                          \
+      Vn.a = fma2(CB, Bc.a, fma2(CA, Ac.a, mul2(CSx.a, w.a)));                                \
+      Vn.b = fma2(CB, Bc.b, fma2(CA, Ac.b, mul2(CSx.b, w.b)));                                \
+      if (EDGE) {                                                                             \
+        const float2 rv = f2((q >= 0 && q < ny) ? 1.f : 0.f);                                 \
+        Vn.a = mul2(Vn.a, rv);                                                                \
+        Vn.b = mul2(Vn.b, rv);                                                                \
+      }                                                                                       \
+      if (io && q >= r0 && q < r1) f4_store(pJ + q * P, Vn);                                  \
+    }                                                                                         \
+    {                                                                                         \
+      const int r = q - 1;                                                                    \
+      const float lft = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                             \
+      if (r >= r0 && r < r1) {                                                                \
+        F4 miss = xmiss;                                                                      \
+        if (EDGE) {                                                                           \
+          const float2 rm = f2(float((r == 0) + (r == ny - 1)));                              \
+          miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                    \
+        }                                                                                     \
+        F4 z = lap4(Vm, Vc, Vn, lft, rgt, miss);                                              \
+        z.a = mul2(z.a, OPx.a);                                                               \
+        z.b = mul2(z.b, OPx.b);                                                               \
+        q0 = fma2(z.a, Am.a, fma2(z.b, Am.b, q0));                                            \
+        q1 = fma2(z.a, Vc.a, fma2(z.b, Vc.b, q1));                                            \
+        q2 = fma2(Am.a, Vc.a, fma2(Am.b, Vc.b, q2));                                          \
+        q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                              \
+        q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
+        q5 = fma2(Am.a, Am.a, fma2(Am.b, Am.b, q5));                                          \
+      }                                                                                       \
+    }                                                                                         \
+    if (FLUSH) {                                                                              \
+      acc[0] += (double)(q0.x + q0.y);                                                        \
+      acc[1] += (double)(q1.x + q1.y);                                                        \
+      acc[2] += (double)(q2.x + q2.y);                                                        \
+      acc[3] += (double)(q3.x + q3.y);                                                        \
+      acc[4] += (double)(q4.x + q4.y);                                                        \
+      acc[5] += (double)(q5.x + q5.y);                                                        \
+      q0 = q1 = q2 = q3 = q4 = q5 = f2(0.f);                                                  \
+    }                                                                                         \
+    Af = rowA(q + 5);                                                                         \
+    Bc = rowB(q + 3);                                                                         \
+  }
+  for (int it0 = 0; it0 < nit; it0 += 6) {
+    int it = it0;
+    NLSB_ROW2(A0, A1, A2, A0, B0, V1, V2, V0, false) ++it;
+    NLSB_ROW2(A1, A2, A3, A1, B1, V2, V0, V1, false) ++it;
+    NLSB_ROW2(A2, A3, A4, A2, B2, V0, V1, V2, true) ++it;
+    NLSB_ROW2(A3, A4, A5, A3, B0, V1, V2, V0, false) ++it;
+    NLSB_ROW2(A4, A5, A0, A4, B1, V2, V0, V1, false) ++it;
+    NLSB_ROW2(A5, A0, A1, A5, B2, V0, V1, V2, true)
+  }
+#undef NLSB_ROW2
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32b(StepArgs a) {
+  using E = float;
+  WARP_TILE_PROLOGUE
+  const int j = a.j, sq = t.local & 1;
+  const float opsc = float(a.op_sign * s.inv_h2);
+  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+  const double b0 = a.beta0[t.slot * 2 + sq];
+  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
+  const float cs = float(sA * L.inv_b) * opsc;
+  const float2 CA = f2(float(-L.ar * sA * L.inv_b)), CB = f2(float(-L.dr * sB * L.inv_b));
+  const long long vo = (long long)sq * a.kv;
+  const bool hasB = j >= 2;
+  const long long lane_off = s.off + S.col0;
+  const float *pA = (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
+  const float *pB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
+  float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
+  // per-element column masks folded into the stencil coefficients, and the
+  // missing-neighbour counts of the x direction
+  F4 CSx, OPx, xmiss;
+  {
+    float v[4], m[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == S.nx - 1));
+    }
+    CSx = F4{make_float2(v[0] * cs, v[1] * cs), make_float2(v[2] * cs, v[3] * cs)};
+    OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
+    xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  const bool ld = S.lane_in, io = S.out_lane;
+  const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (r0 >= 2 && r1 <= ny - 2)
+    lz1f32_march<false>(pA, pB, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc);
+  else
+    lz1f32_march<true>(pA, pB, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc);
+  // the stored V_{j-1} is s0 v_{j-1} at j = 1 (V_0 holds the raw start vector)
+  acc[0] *= sA;
+  acc[2] *= sA;
+  acc[5] *= sA * sA;
+  constexpr int ND = 6;
+  double vals[ND];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
+  const int tc = s.tile_count, TT = *a.lt_stride;
+  if (warp_publish<ND>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot * 2 + sq,
+                       tc, lane)) {
+    const double *part = a.part + (long long)j * a.part_stride;
+    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin, tc, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
+      a.ticket[t.slot * 2 + sq] = 0;
+    }
+  }
+}
+
 // ---------------------- TMA-pipelined FP32 Lanczos pass (2-D, c == 1)
 // One block (4 warps) per (slot, sequence, column tile of <= 512 columns, row
 // segment). Thread 0 streams the rows of V_{j-1} and V_{j-2} with 1-D bulk
