@@ -88,6 +88,7 @@ struct Launch {
   LaunchFn first[2] = {nullptr, nullptr};
   LaunchFn lanczos[2] = {nullptr, nullptr};
   LaunchFn final_[2] = {nullptr, nullptr};
+  bool first_lt[2] = {false, false};  // the first pass runs on the pass tile table
 };
 
 template <typename E, int SRC, bool HC>
@@ -137,6 +138,19 @@ cudaError_t launch2_lanczos1_f32b(const StepArgs &a, int tiles, cudaStream_t st)
     k2_lanczos1_f32b<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
+// Packed FP32 first pass (one warp per strip and sequence); NLS_F32_FIRST=0
+// selects the generic two-sequence kernel.
+bool f32_first_packed() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_F32_FIRST");
+    return (e && std::atoi(e) == 0) ? 0 : 1;
+  }();
+  return v != 0;
+}
+cudaError_t launch2_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_first_f32<<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
 cudaError_t launch2t_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   k2t_lanczos_f32<<<tiles, 128, sizeof(TmaSmem), st>>>(a);
   return cudaGetLastError();
@@ -183,9 +197,26 @@ template <int DIM, typename R> cudaError_t launch_sv(const StepArgs &a, int grid
   k_sv<DIM, R><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_sv<DIM, R>(), st>>>(a);
   return cudaGetLastError();
 }
+// f(T): the register-resident kernel for k <= 16, the shared-memory one above
+// (NLS_FTRI=smem forces the latter).
+bool ftri_smem_only() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_FTRI");
+    return (e && std::strcmp(e, "smem") == 0) ? 1 : 0;
+  }();
+  return v != 0;
+}
 template <typename E> cudaError_t launch_ftri(const StepArgs &a, int nslots_cap, cudaStream_t st) {
   const int warps = nslots_cap * a.nseq;
-  k_ftri<E><<<(warps + 3) / 4, 128, 0, st>>>(a);
+  const int blocks = (warps + 3) / 4;
+  if (ftri_smem_only() || a.k > 16)
+    k_ftri<E><<<blocks, 128, 0, st>>>(a);
+  else if (a.k <= 8)
+    k_ftri_reg<E, 8><<<blocks, 128, 0, st>>>(a);
+  else if (a.k <= 12)
+    k_ftri_reg<E, 12><<<blocks, 128, 0, st>>>(a);
+  else
+    k_ftri_reg<E, 16><<<blocks, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 template <typename E, int KIND>
@@ -267,6 +298,10 @@ template <typename R> KSet make_real2() {
   k.kg.lanczos[1] = launch2_lanczos1<R, true>;
   if constexpr (sizeof(R) == 4) {
     k.kg.lanczos[0] = f32_pass_form() == 1 ? launch2_lanczos1_f32 : launch2_lanczos1_f32b;  // packed FP32x2
+    if (f32_first_packed()) {
+      k.kg.first[0] = launch2_first_f32;
+      k.kg.first_lt[0] = true;
+    }
     k.lanczos_tma = launch2t_lanczos_f32;
     k.set_attrs = attrs_tma_f32;
   }
@@ -695,7 +730,15 @@ StepArgs base_args(const nls_pool *P, const TileSet &T) {
 // One Krylov application family (first pass, Lanczos passes, f(T), final).
 int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &nk) {
   const int grid = T.cap, hc = P->step_hc;
-  CK(L.first[hc](a, grid, P->stream));
+  if (L.first_lt[hc]) {
+    StepArgs f = a;
+    f.tiles = T.d_lt;
+    f.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
+    f.lt_stride = T.d_nlt1;
+    CK(L.first[hc](f, T.lcap, P->stream));
+  } else {
+    CK(L.first[hc](a, grid, P->stream));
+  }
   ++nk;
   StepArgs b = a;  // 2-D passes: one warp per (strip, sequence) or one TMA block per tile
   int lgrid = grid;

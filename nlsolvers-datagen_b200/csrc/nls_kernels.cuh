@@ -694,6 +694,222 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   }
 }
 
+// Register-resident f(T) for k <= KP (KP = 8, 12, 16): the same T assembly,
+// implicit QL sweeps and coefficients as k_ftri, but every lane of the warp
+// runs the scalar QL recurrences itself on register copies of d and e (the
+// loops are unrolled to KP with the active range as a warp-uniform predicate,
+// so all indices are static) and applies each Givens rotation to its own row
+// `lane` of the eigenvector matrix immediately: no shared memory, no per-sweep
+// synchronisation.
+template <typename E, int KP>
+__global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
+  constexpr bool CP = Traits<E>::cplx;
+  using R = typename Traits<E>::R;
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int li = gw / a.nseq, sq = gw % a.nseq;
+  if (li >= *a.nslot_list) return;
+  const int slot = a.slot_list[li];
+  const SlotDesc &s = a.slots[slot];
+  const int k = a.k, jl = k - 2;
+  constexpr int ND = CP ? 9 : 6;
+  LzScal Lk;
+  if (a.scal_ready) {
+    Lk = a.scal[(slot * 2 + sq) * KMAX + jl];
+  } else {
+    const int NV = ND * a.nseq;
+    double tot = 0.0;
+    if (lane < ND) {
+      const double *pp = a.part + (long long)jl * a.part_stride;
+      for (int t = 0; t < s.tile_count; ++t) tot += pp[(long long)(s.tile_begin + t) * NV + sq * ND + lane];
+    }
+    double tv[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    Lk = lz_from_dots<CP>(tv, Eps<R>::v);
+  }
+  // lane j < k-1 holds alpha_j and the subdiagonal entry T[j, j-1] (lanczos.hpp:217-239)
+  double my_a = 0.0, my_sr = 0.0, my_si = 0.0;
+  if (lane <= jl) {
+    const LzScal L = lane == jl ? Lk : a.scal[(slot * 2 + sq) * KMAX + lane];
+    my_a = L.ar;
+    if (lane >= 1) {
+      my_sr = L.dr;
+      my_si = L.di;
+    }
+  } else if (lane == k - 1) {
+    my_sr = Lk.b;
+  }
+  double d[KP], e[KP];
+  double pr = 1.0, pi = 0.0, my_pr = 1.0, my_pi = 0.0;  // phase delta_lane
+#pragma unroll
+  for (int j = 0; j < KP; ++j) {
+    const double aj = __shfl_sync(0xffffffffu, my_a, j);
+    const double sr = __shfl_sync(0xffffffffu, my_sr, j), si = __shfl_sync(0xffffffffu, my_si, j);
+    d[j] = j < k - 1 ? aj : 0.0;
+    e[j] = 0.0;
+    if (j >= 1 && j < k) {
+      const double mag = sqrt(sr * sr + si * si);
+      e[j - 1] = mag;
+      if (mag > 0.0) {
+        const double ur = sr / mag, ui = si / mag;
+        const double nr = pr * ur - pi * ui, ni = pr * ui + pi * ur;
+        pr = nr;
+        pi = ni;
+      }
+      if (j == lane) {
+        my_pr = pr;
+        my_pi = pi;
+      }
+    }
+  }
+  double Z[KP];
+#pragma unroll
+  for (int i = 0; i < KP; ++i) Z[i] = i == lane ? 1.0 : 0.0;
+  int status = 0;
+#pragma unroll
+  for (int l = 0; l < KP; ++l) {
+    if (l >= k || status) break;
+    for (int iter = 0;; ++iter) {
+      int m = k - 1;
+      bool found = false;
+#pragma unroll
+      for (int mm = l; mm < KP - 1; ++mm) {
+        if (!found && mm < k - 1) {
+          const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+          if (fabs(e[mm]) <= 2.220446049250313e-16 * dd) {
+            m = mm;
+            found = true;
+          }
+        }
+      }
+      if (m == l) break;
+      if (iter >= 60) {
+        status = -1;
+        break;
+      }
+      const int l1 = l + 1 < KP ? l + 1 : KP - 1;  // m > l, so l + 1 < KP when reached
+      double dm = 0.0;
+#pragma unroll
+      for (int q = 0; q < KP; ++q)
+        if (q == m) dm = d[q];
+      double g = (d[l1] - d[l]) / (2.0 * e[l]);
+      double r = sqrt(g * g + 1.0);
+      g = dm - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+      double sn = 1.0, cs = 1.0, p = 0.0;
+      bool defl = false;
+#pragma unroll
+      for (int i = KP - 2; i >= l; --i) {
+        if (i <= m - 1 && !defl) {
+          const double f = sn * e[i];
+          const double b = cs * e[i];
+          const double t2 = f * f + g * g;
+          if (t2 == 0.0) {
+            e[i + 1] = 0.0;
+            d[i + 1] -= p;
+            defl = true;
+          } else {
+            const double ir = rsqrt(t2);
+            r = t2 * ir;
+            e[i + 1] = r;
+            sn = f * ir;
+            cs = g * ir;
+            g = d[i + 1] - p;
+            r = (d[i] - g) * sn + 2.0 * cs * b;
+            p = sn * r;
+            d[i + 1] = g + p;
+            g = cs * r - b;
+            // rotate columns i, i+1 of this lane's row
+            const double zi = Z[i], zi1 = Z[i + 1];
+            Z[i + 1] = sn * zi + cs * zi1;
+            Z[i] = cs * zi - sn * zi1;
+          }
+        }
+      }
+      if (defl) {
+#pragma unroll
+        for (int q = 0; q < KP; ++q)
+          if (q == m) e[q] = 0.0;
+      } else {
+        d[l] -= p;
+        e[l] = g;
+#pragma unroll
+        for (int q = 0; q < KP; ++q)
+          if (q == m) e[q] = 0.0;
+      }
+    }
+  }
+  // f(lambda_i) Z[0][i] for i = lane, then c_r = delta_r sum_i Z[r][i] f_i Z[0][i]
+  const int fk = a.fkind[sq];
+  double lam = 0.0, z0 = 0.0;
+#pragma unroll
+  for (int i = 0; i < KP; ++i) {
+    const double zi0 = __shfl_sync(0xffffffffu, Z[i], 0);
+    if (i == lane) {
+      lam = d[i];
+      z0 = zi0;
+    }
+  }
+  double fr = 0.0, fi = 0.0;
+  if (lane < k) {
+    fval(fk, lam, a.tsc[sq][0] * s.dt, a.tsc[sq][1] * s.dt, fr, fi);
+    fr *= z0;
+    fi *= z0;
+  }
+  double cr = 0.0, ci = 0.0;
+#pragma unroll
+  for (int i = 0; i < KP; ++i) {
+    const double gr = __shfl_sync(0xffffffffu, fr, i), gi = __shfl_sync(0xffffffffu, fi, i);
+    if (i < k) {
+      cr += gr * Z[i];
+      ci += gi * Z[i];
+    }
+  }
+  {
+    const double tr = my_pr * cr - my_pi * ci, ti = my_pr * ci + my_pi * cr;
+    cr = tr;
+    ci = ti;
+    if (lane == 0 && a.incr[sq]) cr -= 1.0;
+  }
+  FinalCoef &F = a.coef[slot * 2 + sq];
+  const double beta0 = a.beta0[slot * 2 + sq];
+  const double s0 = beta0 > 0.0 ? 1.0 / beta0 : 0.0;
+  const double sA = (jl == 0) ? s0 : 1.0;
+  const double sB = (jl - 1 == 0) ? s0 : 1.0;
+  double wr = 0.0, wi = 0.0;
+  if (lane < k - 1) {
+    const double sj = lane == 0 ? s0 : 1.0;
+    wr = beta0 * sj * cr;
+    wi = beta0 * sj * ci;
+  }
+  const double lr = __shfl_sync(0xffffffffu, cr, k - 1) * beta0 * Lk.inv_b;
+  const double lim = __shfl_sync(0xffffffffu, ci, k - 1) * beta0 * Lk.inv_b;
+  if (lane == k - 2) {
+    wr -= sA * (lr * Lk.ar - lim * Lk.ai);
+    wi -= sA * (lr * Lk.ai + lim * Lk.ar);
+  }
+  if (lane == k - 3) {
+    wr -= sB * (lr * Lk.dr - lim * Lk.di);
+    wi -= sB * (lr * Lk.di + lim * Lk.dr);
+  }
+  if (lane < k - 1) {
+    F.wr[lane] = wr;
+    F.wi[lane] = wi;
+    F.wr32[lane] = (float)wr;
+    F.wi32[lane] = (float)wi;
+  }
+  if (lane == 0) {
+    F.lam_r = lr * sA;
+    F.lam_i = lim * sA;
+    F.lam32[0] = (float)(lr * sA);
+    F.lam32[1] = (float)(lim * sA);
+    F.beta0 = beta0;
+    F.kv = k - 1;
+    a.scal[(slot * 2 + sq) * KMAX + jl] = Lk;
+    if (status) a.state[slot].status = -8;
+  }
+}
+
 #include "nls_kernels_tail.cuh"
 #include "nls_warp2d.cuh"
 

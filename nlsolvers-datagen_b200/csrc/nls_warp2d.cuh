@@ -1478,6 +1478,147 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32b(StepArgs a) {
   }
 }
 
+// Packed FP32 first pass for KG / phi^4 (c == 1): one warp per (strip,
+// sequence) of the pass tile table; sequence 0 starts from x = u, sequence 1
+// from x = g(u) = (p1 m + q1) u + (p3 m + q3) u^3 (+ (rm m + r0) xi). Stores
+// V_0 = x, z = A x, and the three dots the first Lanczos step needs
+// (<z,x>, |z|^2, |x|^2) in the six-value layout of the passes. Rows of u (and
+// m) are prefetched four rows ahead; interior segments run without row masks.
+__device__ __forceinline__ F4 f4_g(const F4 &u, const F4 &m, float2 P1, float2 Q1, float2 P3, float2 Q3) {
+  const float2 a1 = fma2(P1, m.a, Q1), b1 = fma2(P1, m.b, Q1);
+  const float2 a3 = fma2(P3, m.a, Q3), b3 = fma2(P3, m.b, Q3);
+  const float2 ua3 = mul2(mul2(u.a, u.a), u.a), ub3 = mul2(mul2(u.b, u.b), u.b);
+  return F4{fma2(a1, u.a, mul2(a3, ua3)), fma2(b1, u.b, mul2(b3, ub3))};
+}
+
+template <bool EDGE, int SQ>
+__device__ __forceinline__ void first_f32_march(const float *pU, const float *pM, float *pV, int P, int r0, int r1,
+                                                int ny, bool ld, bool io, const SlotDesc &s, const Strip &S,
+                                                int step, const F4 &OPx, const F4 &xmiss, double *acc) {
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  const float2 P1 = f2(float(s.p1)), Q1 = f2(float(s.q1)), P3 = f2(float(s.p3)), Q3 = f2(float(s.q3));
+  const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
+  auto rowU = [&](int r) -> F4 {
+    const bool ok = EDGE ? (ld && r >= 0 && r < ny && r <= r1) : (ld && r <= r1);
+    return ok ? f4_load(pU + r * P) : zero4;
+  };
+  auto rowM = [&](int r) -> F4 {
+    if (SQ == 0) return zero4;
+    const bool ok = EDGE ? (ld && r >= 0 && r < ny && r <= r1) : (ld && r <= r1);
+    return ok ? f4_load(pM + r * P) : zero4;
+  };
+  // source row r from its raw rows (g and noise for sequence 1; zero outside the grid)
+  auto make = [&](const F4 &u, const F4 &m, int r) -> F4 {
+    if (SQ == 0) return u;
+    F4 x = f4_g(u, m, P1, Q1, P3, Q3);
+    if (noisy && r >= 0 && r < ny) {
+      float xs[4] = {x.a.x, x.a.y, x.b.x, x.b.y};
+      const float ms[4] = {m.a.x, m.a.y, m.b.x, m.b.y};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int xx = S.col0 + e;
+        if (xx >= 0 && xx < S.nx)
+          xs[e] += (float(s.rm) * ms[e] + float(s.r0)) *
+                   philox_normal<float>(s.seed, (uint32_t)step, (uint32_t)((long long)r * S.nx + xx));
+      }
+      x = F4{make_float2(xs[0], xs[1]), make_float2(xs[2], xs[3])};
+    }
+    return x;
+  };
+  float2 q1 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
+  // x rows r0-1, r0 made; raw rows r0+1 .. r0+4 in flight
+  F4 X0 = make(rowU(r0 - 1), rowM(r0 - 1), r0 - 1), X1 = make(rowU(r0), rowM(r0), r0), X2 = zero4, X3 = zero4;
+  F4 U0 = rowU(r0 + 1), U1 = rowU(r0 + 2), U2 = rowU(r0 + 3), U3 = rowU(r0 + 4);
+  F4 M0 = rowM(r0 + 1), M1 = rowM(r0 + 2), M2 = rowM(r0 + 3), M3 = rowM(r0 + 4);
+  const int nit = (r1 - r0 + 3) / 4 * 4;
+#define NLSB_FIRST(Xm, Xc, Xp, Uc, Mc)                                                     \
+  {                                                                                        \
+    const int c = r0 + it;                                                                 \
+    Xp = make(Uc, Mc, c + 1);                                                              \
+    Uc = rowU(c + 5);                                                                      \
+    Mc = rowM(c + 5);                                                                      \
+    const float lft = __shfl_up_sync(0xffffffffu, Xc.b.y, 1);                              \
+    const float rgt = __shfl_down_sync(0xffffffffu, Xc.a.x, 1);                            \
+    if (c < r1) {                                                                          \
+      F4 miss = xmiss;                                                                     \
+      if (EDGE) {                                                                          \
+        const float2 rm = f2(float((c == 0) + (c == ny - 1)));                             \
+        miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                   \
+      }                                                                                    \
+      F4 z = lap4(Xm, Xc, Xp, lft, rgt, miss);                                             \
+      z.a = mul2(z.a, OPx.a);                                                              \
+      z.b = mul2(z.b, OPx.b);                                                              \
+      if (io) f4_store(pV + c * P, Xc);                                                    \
+      q1 = fma2(z.a, Xc.a, fma2(z.b, Xc.b, q1));                                           \
+      q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                             \
+      q4 = fma2(Xc.a, Xc.a, fma2(Xc.b, Xc.b, q4));                                         \
+    }                                                                                      \
+  }
+  for (int it0 = 0; it0 < nit; it0 += 4) {
+    int it = it0;
+    NLSB_FIRST(X0, X1, X2, U0, M0) ++it;
+    NLSB_FIRST(X1, X2, X3, U1, M1) ++it;
+    NLSB_FIRST(X2, X3, X0, U2, M2) ++it;
+    NLSB_FIRST(X3, X0, X1, U3, M3)
+    acc[1] += (double)(q1.x + q1.y);
+    acc[3] += (double)(q3.x + q3.y);
+    acc[4] += (double)(q4.x + q4.y);
+    q1 = q3 = q4 = f2(0.f);
+  }
+#undef NLSB_FIRST
+}
+
+static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
+  using E = float;
+  WARP_TILE_PROLOGUE
+  const int sq = t.local & 1;
+  const float opsc = float(a.op_sign * s.inv_h2);
+  F4 OPx, xmiss;
+  {
+    float v[4], m[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == S.nx - 1));
+    }
+    OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
+    xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  const long long lane_off = s.off + S.col0;
+  const float *pU = (const float *)a.f.u_hi + lane_off;
+  const float *pM = (const float *)a.f.m + lane_off;
+  float *pV = (float *)a.V + (long long)(sq * a.kv) * a.vstride + lane_off;
+  const bool ld = S.lane_in, io = S.out_lane;
+  const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const bool inner = r0 >= 2 && r1 <= ny - 2;
+  if (sq == 0) {
+    if (inner) first_f32_march<false, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
+    else first_f32_march<true, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
+  } else {
+    if (inner) first_f32_march<false, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
+    else first_f32_march<true, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
+  }
+  constexpr int ND = 6;
+  double vals[ND];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
+  const int tc = s.tile_count, TT = *a.lt_stride;
+  if (warp_publish<ND>(vals, a.part, wt, a.ticket + t.slot * 2 + sq, tc, lane)) {
+    const double tot = warp_slot_total<ND>(a.part, sq * TT + s.tile_begin, tc, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      double b0;
+      a.scal[(t.slot * 2 + sq) * KMAX + 0] = lz_first<false>(tv, Eps<float>::v, b0);
+      a.beta0[t.slot * 2 + sq] = b0;
+      a.ticket[t.slot * 2 + sq] = 0;
+    }
+  }
+}
+
 // ---------------------- TMA-pipelined FP32 Lanczos pass (2-D, c == 1)
 // One block (4 warps) per (slot, sequence, column tile of <= 512 columns, row
 // segment). Thread 0 streams the rows of V_{j-1} and V_{j-2} with 1-D bulk
