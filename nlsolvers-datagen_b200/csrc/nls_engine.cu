@@ -123,13 +123,26 @@ cudaError_t launch2_lanczos1_f32(const StepArgs &a, int tiles, cudaStream_t st) 
   return cudaGetLastError();
 }
 // Packed FP32 pass form: 2 (default) interior fast path + FP64 dot flushes,
-// 1 the first form (per-row Kahan, row masks everywhere); NLS_F32_PASS selects.
+// 1 the first form (per-row Kahan, row masks everywhere), 3 the form with a
+// per-warp cp.async shared-memory row ring; NLS_F32_PASS selects.
 int f32_pass_form() {
   static int v = [] {
     const char *e = std::getenv("NLS_F32_PASS");
-    return (e && std::atoi(e) == 1) ? 1 : 2;
+    const int f = e ? std::atoi(e) : 2;
+    return (f == 1 || f == 3) ? f : 2;
   }();
   return v;
+}
+cudaError_t launch2_lanczos1_f32c(const StepArgs &a, int tiles, cudaStream_t st) {
+  static const int minb = [] {
+    const char *e = std::getenv("NLS_F32C_BLOCKS");
+    return (e && std::atoi(e) == 5) ? 5 : 4;
+  }();
+  if (minb == 5)
+    k2_lanczos1_f32c<5><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  else
+    k2_lanczos1_f32c<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
 }
 cudaError_t launch2_lanczos1_f32b(const StepArgs &a, int tiles, cudaStream_t st) {
   if (f32_minb() == 3)
@@ -297,7 +310,9 @@ template <typename R> KSet make_real2() {
   k.kg.lanczos[0] = launch2_lanczos1<R, false>;
   k.kg.lanczos[1] = launch2_lanczos1<R, true>;
   if constexpr (sizeof(R) == 4) {
-    k.kg.lanczos[0] = f32_pass_form() == 1 ? launch2_lanczos1_f32 : launch2_lanczos1_f32b;  // packed FP32x2
+    k.kg.lanczos[0] = f32_pass_form() == 1   ? launch2_lanczos1_f32
+                      : f32_pass_form() == 3 ? launch2_lanczos1_f32c
+                                             : launch2_lanczos1_f32b;  // packed FP32x2
     if (f32_first_packed()) {
       k.kg.first[0] = launch2_first_f32;
       k.kg.first_lt[0] = true;

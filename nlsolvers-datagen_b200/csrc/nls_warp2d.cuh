@@ -1478,6 +1478,179 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32b(StepArgs a) {
   }
 }
 
+// Third form of the packed FP32 pass: the rows of V_{j-1} and V_{j-2} are
+// streamed by each lane's own 16-byte cp.async copies into a per-warp
+// shared-memory ring CPD rows ahead. Rows in flight cost no registers and no
+// barrier is needed (a lane reads back only the cells it copied; x-neighbours
+// still come through shuffles), so more warps fit per SM and each keeps CPD
+// rows of both vectors in flight. Rows outside the grid or past the segment
+// are zero-filled by the copy itself (source size 0).
+constexpr int CPD = 8;
+__device__ __forceinline__ void cp16z(uint32_t sdst, const void *g, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sdst), "l"(g), "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ F4 lds16(uint32_t saddr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(saddr));
+  return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB, const float *safe, float *pJ, int P,
+                                                int r0, int r1, int ny, bool ld, bool io, bool hasB, float2 CA,
+                                                float2 CB, const F4 &CSx, const F4 &OPx, const F4 &xmiss,
+                                                double *acc, uint32_t cellA, uint32_t cellB) {
+  // fetch f: A row r0-2+f into slot f % CPD of ring A, B row r0-2+f into ring B
+  // (fetch 0 of B is never read); one commit group per fetch
+  auto fetch = [&](int f) {
+    const int r = r0 - 2 + f;
+    const uint32_t off = (uint32_t)((f % CPD) * 512);
+    const bool okA = EDGE ? (ld && r >= 0 && r < ny && r <= r1 + 1) : (ld && r <= r1 + 1);
+    const bool okB = EDGE ? (ld && hasB && f >= 1 && r >= 0 && r < ny && r <= r1) : (ld && hasB && f >= 1 && r <= r1);
+    cp16z(cellA + off, okA ? (const void *)(pA + r * P) : (const void *)safe, okA);
+    cp16z(cellB + off, okB ? (const void *)(pB + r * P) : (const void *)safe, okB);
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int f = 0; f < CPD; ++f) fetch(f);
+  cp_async_wait<CPD - 2>();
+  F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2;
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  F4 V0 = zero4, V1 = zero4, V2 = zero4, Bq;
+  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f), q5 = f2(0.f);
+  const int qb = r0 - 1;
+  const int nit = ((r1 - qb + 1) + 2) / 3 * 3;
+#define NLSB_ROW3(Am, Ac, Ap, Vm, Vc, Vn)                                                       \
+  {                                                                                           \
+    const int q = qb + it;                                                                    \
+    cp_async_wait<CPD - 3>();                                                                 \
+    Ap = lds16(cellA + (uint32_t)(((it + 2) % CPD) * 512));                                   \
+    Bq = lds16(cellB + (uint32_t)(((it + 1) % CPD) * 512));                                   \
+    fetch(it + CPD);                                                                          \
+    {                                                                                         \
+      const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
+      F4 miss = xmiss;                                                                        \
+      if (EDGE) {                                                                             \
+        const float2 rm = f2(float((q == 0) + (q == ny - 1)));                                \
+        miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                      \
+      }                                                                                       \
+      const F4 w = lap4(Am, Ac, Ap, lft, rgt, miss);                                          \
+      Vn.a = fma2(CB, Bq.a, fma2(CA, Ac.a, mul2(CSx.a, w.a)));                                \
+      Vn.b = fma2(CB, Bq.b, fma2(CA, Ac.b, mul2(CSx.b, w.b)));                                \
+      if (EDGE) {                                                                             \
+        const float2 rv = f2((q >= 0 && q < ny) ? 1.f : 0.f);                                 \
+        Vn.a = mul2(Vn.a, rv);                                                                \
+        Vn.b = mul2(Vn.b, rv);                                                                \
+      }                                                                                       \
+      if (io && q >= r0 && q < r1) f4_store(pJ + q * P, Vn);                                  \
+    }                                                                                         \
+    {                                                                                         \
+      const int r = q - 1;                                                                    \
+      const float lft = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                             \
+      if (r >= r0 && r < r1) {                                                                \
+        F4 miss = xmiss;                                                                      \
+        if (EDGE) {                                                                           \
+          const float2 rm = f2(float((r == 0) + (r == ny - 1)));                              \
+          miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                    \
+        }                                                                                     \
+        F4 z = lap4(Vm, Vc, Vn, lft, rgt, miss);                                              \
+        z.a = mul2(z.a, OPx.a);                                                               \
+        z.b = mul2(z.b, OPx.b);                                                               \
+        q0 = fma2(z.a, Am.a, fma2(z.b, Am.b, q0));                                            \
+        q1 = fma2(z.a, Vc.a, fma2(z.b, Vc.b, q1));                                            \
+        q2 = fma2(Am.a, Vc.a, fma2(Am.b, Vc.b, q2));                                          \
+        q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                              \
+        q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
+        q5 = fma2(Am.a, Am.a, fma2(Am.b, Am.b, q5));                                          \
+      }                                                                                       \
+    }                                                                                         \
+  }
+  for (int it0 = 0; it0 < nit; it0 += 3) {
+    int it = it0;
+    NLSB_ROW3(A0, A1, A2, V1, V2, V0) ++it;
+    NLSB_ROW3(A1, A2, A0, V2, V0, V1) ++it;
+    NLSB_ROW3(A2, A0, A1, V0, V1, V2)
+    acc[0] += (double)(q0.x + q0.y);
+    acc[1] += (double)(q1.x + q1.y);
+    acc[2] += (double)(q2.x + q2.y);
+    acc[3] += (double)(q3.x + q3.y);
+    acc[4] += (double)(q4.x + q4.y);
+    acc[5] += (double)(q5.x + q5.y);
+    q0 = q1 = q2 = q3 = q4 = q5 = f2(0.f);
+  }
+#undef NLSB_ROW3
+  cp_async_wait<0>();
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
+  using E = float;
+  __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
+  WARP_TILE_PROLOGUE
+  const int j = a.j, sq = t.local & 1;
+  const float opsc = float(a.op_sign * s.inv_h2);
+  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+  const double b0 = a.beta0[t.slot * 2 + sq];
+  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
+  const float cs = float(sA * L.inv_b) * opsc;
+  const float2 CA = f2(float(-L.ar * sA * L.inv_b)), CB = f2(float(-L.dr * sB * L.inv_b));
+  const long long vo = (long long)sq * a.kv;
+  const bool hasB = j >= 2;
+  const float *base = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
+  const long long lane_off = s.off + S.col0;
+  const float *pA = (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
+  const float *pB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
+  float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
+  F4 CSx, OPx, xmiss;
+  {
+    float v[4], m[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == S.nx - 1));
+    }
+    CSx = F4{make_float2(v[0] * cs, v[1] * cs), make_float2(v[2] * cs, v[3] * cs)};
+    OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
+    xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  const int wib = threadIdx.x >> 5;
+  const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&ring[wib][0][0][lane * 16]);
+  const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&ring[wib][1][0][lane * 16]);
+  const bool ld = S.lane_in, io = S.out_lane;
+  const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (r0 >= 2 && r1 <= ny - 2)
+    lz1f32_cp_march<false>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA, cellB);
+  else
+    lz1f32_cp_march<true>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA, cellB);
+  acc[0] *= sA;
+  acc[2] *= sA;
+  acc[5] *= sA * sA;
+  constexpr int ND = 6;
+  double vals[ND];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
+  const int tc = s.tile_count, TT = *a.lt_stride;
+  if (warp_publish<ND>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot * 2 + sq,
+                       tc, lane)) {
+    const double *part = a.part + (long long)j * a.part_stride;
+    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin, tc, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
+      a.ticket[t.slot * 2 + sq] = 0;
+    }
+  }
+}
+
 // Packed FP32 first pass for KG / phi^4 (c == 1): one warp per (strip,
 // sequence) of the pass tile table; sequence 0 starts from x = u, sequence 1
 // from x = g(u) = (p1 m + q1) u + (p3 m + q3) u^3 (+ (rm m + r0) xi). Stores
