@@ -346,7 +346,7 @@ def run_ours(args, ws, rank, lrank):
                    "l2": "working set 0.6 GB per GPU >> 126 MB L2 (no flush needed)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k2_lanczos1_f32 (2-D FP32 Lanczos pass j=2)",
+                     "kernel": "k2_lanczos1_f32c (2-D FP32 Lanczos pass j=2)",
                      "bytes_per_launch": pass_bytes, "launch_ms": pass_ms},
         "step_roofline": {"algorithmic_bytes_per_gp_step": step_bytes_per_gp(k),
                           "achieved_GBps": step_bytes * args.steps / (ms / 1e3) / 1e9 * 1.0,

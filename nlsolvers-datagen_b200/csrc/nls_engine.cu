@@ -122,14 +122,14 @@ cudaError_t launch2_lanczos1_f32(const StepArgs &a, int tiles, cudaStream_t st) 
     k2_lanczos1_f32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
-// Packed FP32 pass form: 2 (default) interior fast path + FP64 dot flushes,
-// 1 the first form (per-row Kahan, row masks everywhere), 3 the form with a
-// per-warp cp.async shared-memory row ring; NLS_F32_PASS selects.
+// Packed FP32 pass form: 3 (default) per-warp cp.async shared-memory row ring;
+// 2 register rings with the interior fast path and FP64 dot flushes; 1 the
+// first form (per-row Kahan, row masks everywhere). NLS_F32_PASS selects.
 int f32_pass_form() {
   static int v = [] {
     const char *e = std::getenv("NLS_F32_PASS");
-    const int f = e ? std::atoi(e) : 2;
-    return (f == 1 || f == 3) ? f : 2;
+    const int f = e ? std::atoi(e) : 3;
+    return (f == 1 || f == 2) ? f : 3;
   }();
   return v;
 }
