@@ -191,13 +191,18 @@ __device__ __forceinline__ bool warp_publish(double *vals, double *part, int til
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     vals[q] = v;
   }
+  int last = 0;
   if (lane == 0) {
 #pragma unroll
     for (int q = 0; q < NVAL; ++q) __stcg(part + (long long)tile * NVAL + q, vals[q]);
+    // release: this lane's partial stores are visible before its ticket;
+    // acquire: the last arrival observes every earlier warp's partials. The
+    // other lanes' stores (the tile's rows) need no ordering with the ticket.
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;\n" : "=r"(old) : "l"(ticket) : "memory");
+    last = old == tile_count - 1;
   }
-  __threadfence();
-  int last = 0;
-  if (lane == 0) last = atomicAdd(ticket, 1) == tile_count - 1;
+  __syncwarp();
   last = __shfl_sync(0xffffffffu, last, 0);
   if (last) __threadfence();
   return last != 0;
@@ -1489,6 +1494,9 @@ constexpr int CPD = 8;
 __device__ __forceinline__ void cp16z(uint32_t sdst, const void *g, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sdst), "l"(g), "r"(valid ? 16 : 0));
 }
+__device__ __forceinline__ void cp16s(uint32_t sdst, const void *g, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sdst), "l"(g), "r"(src_bytes));
+}
 __device__ __forceinline__ F4 lds16(uint32_t saddr) {
   float4 v;
   asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
@@ -1513,8 +1521,30 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
     cp16z(cellB + off, okB ? (const void *)(pB + r * P) : (const void *)safe, okB);
     cp_async_commit();
   };
+  // interior segments: each lane's row pointers advance by the pitch per
+  // fetch; copies past the last row a kept result reads (A: r1+1, B: r1) are
+  // skipped (the test is warp-uniform), so those slots keep stale rows that
+  // only discarded iterations read
+  const float *gA = ld ? pA + (r0 - 2) * P : safe;
+  const float *gB = (ld && hasB) ? pB + (r0 - 2) * P : safe;
+  const int stA = ld ? P : 0, stB = (ld && hasB) ? P : 0;
+  const int szA = ld ? 16 : 0, szB = (ld && hasB) ? 16 : 0;
+  const int fA_last = r1 + 3 - r0, fB_last = r1 + 2 - r0;
+  constexpr uint32_t RM = CPD * 512 - 1;
+  uint32_t soff = 0, ldA = 2 * 512, ldB = 512;
+  auto fetch_fast = [&](int f) {
+    if (f <= fA_last) cp16s(cellA + soff, gA, szA);
+    if (f >= 1 && f <= fB_last) cp16s(cellB + soff, gB, szB);
+    gA += stA;
+    gB += stB;
+    soff = (soff + 512) & RM;
+    cp_async_commit();
+  };
 #pragma unroll
-  for (int f = 0; f < CPD; ++f) fetch(f);
+  for (int f = 0; f < CPD; ++f) {
+    if (EDGE) fetch(f);
+    else fetch_fast(f);
+  }
   cp_async_wait<CPD - 2>();
   F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2;
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
@@ -1526,9 +1556,12 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
   {                                                                                           \
     const int q = qb + it;                                                                    \
     cp_async_wait<CPD - 3>();                                                                 \
-    Ap = lds16(cellA + (uint32_t)(((it + 2) % CPD) * 512));                                   \
-    Bq = lds16(cellB + (uint32_t)(((it + 1) % CPD) * 512));                                   \
-    fetch(it + CPD);                                                                          \
+    Ap = lds16(cellA + ldA);                                                                  \
+    Bq = lds16(cellB + ldB);                                                                  \
+    ldA = (ldA + 512) & RM;                                                                   \
+    ldB = (ldB + 512) & RM;                                                                   \
+    if (EDGE) fetch(it + CPD);                                                                \
+    else fetch_fast(it + CPD);                                                                \
     {                                                                                         \
       const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
       const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
