@@ -144,6 +144,7 @@ int nls_pool_set_graphs(nls_pool *pool, int32_t enable);
 /* Rows of the march segment (tile length along y in 2-D / z in 3-D). */
 int nls_pool_set_segment(nls_pool *pool, int32_t rows);
 /* Time `iters` launches of Lanczos pass j (1 <= j <= k-2) on the current state
+   (over every slot group of the step, launched side by side as the step does)
    with CUDA events; *ms = mean duration of one launch; *points = grid points
    covered by one launch. The pass is idempotent, so the state is unchanged. */
 int nls_pool_time_pass(nls_pool *pool, int32_t j, int32_t iters, float *ms, int64_t *points);

@@ -474,17 +474,24 @@ struct nls_pool {
   double *d_diag_part = nullptr, *d_diag_out = nullptr;  // per slot: k_diag partials / result
   int *d_diag_ticket = nullptr;
   TileSet main, first;  // main step / SEWI Strang first steps
+  // The main step's slots in two groups (main, main2) whose launch sequences
+  // run as parallel branches: one group's latency-bound f(T) and kernel tails
+  // overlap the other group's bandwidth-bound passes.
+  TileSet main2;
+  bool split = false;      // the current tables hold two groups
+  bool split_on = true;    // NLS_SPLIT=0 keeps one group
   std::vector<SlotHost> hs;
   std::vector<SlotDesc> sd;
   bool tables_dirty = true;
   int seg2 = 32, seg3 = 16;
-  cudaStream_t stream = nullptr, copy_stream = nullptr;
-  cudaEvent_t ev_step = nullptr;
+  cudaStream_t stream = nullptr, copy_stream = nullptr, stream2 = nullptr;
+  cudaEvent_t ev_step = nullptr, ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = true;
   cudaGraphExec_t gexec = nullptr;
   int graph_tiles = -1, graph_ring = -1, graph_hc = -1;
   void *graph_part = nullptr;
   int graph_lcap = -1, graph_tcap = -1;
+  int graph_split = -1, graph_tiles2 = -1, graph_lcap2 = -1, graph_tcap2 = -1;
   int step_hc = 0;  // some stepped slot carries a c field
   int ring_blocks = 1;
   int kernels_per_step = 0;
@@ -531,7 +538,9 @@ void pool_free_device(nls_pool *P) {
                   P->first.d_nlist, P->main.d_lt, P->main.d_nlt1, P->main.d_nlt2,
                   P->first.d_lt, P->first.d_nlt1, P->first.d_nlt2, P->main.d_tt,
                   P->main.d_ntt1, P->main.d_ntt2, P->first.d_tt, P->first.d_ntt1,
-                  P->first.d_ntt2, P->zeros, P->d_diag_part, P->d_diag_out, P->d_diag_ticket};
+                  P->first.d_ntt2, P->main2.d_tiles, P->main2.d_ntiles, P->main2.d_list,
+                  P->main2.d_nlist, P->main2.d_lt, P->main2.d_nlt1, P->main2.d_nlt2, P->main2.d_tt,
+                  P->main2.d_ntt1, P->main2.d_ntt2, P->zeros, P->d_diag_part, P->d_diag_out, P->d_diag_ticket};
   for (void *b : bufs)
     if (b) cudaFree(b);
 }
@@ -599,7 +608,8 @@ int ensure_partials(nls_pool *P, int tiles) {
   if (P->part) cudaFree(P->part);
   P->part = nullptr;
   const int passes = std::max(P->k - 1, 1);
-  CK(cudaMalloc(&P->part, sizeof(double) * (size_t)passes * cap * nv));
+  // two regions: one per group of the main step
+  CK(cudaMalloc(&P->part, 2 * sizeof(double) * (size_t)passes * cap * nv));
   P->part_tiles = cap;
   P->gexec ? (void)0 : (void)0;
   return NLS_OK;
@@ -609,16 +619,32 @@ int ensure_partials(nls_pool *P, int tiles) {
 int rebuild_tables(nls_pool *P) {
   P->main.tiles.clear();
   P->main.list.clear();
+  P->main2.tiles.clear();
+  P->main2.list.clear();
   P->first.tiles.clear();
   P->first.list.clear();
   P->step_hc = 0;
   int max_ring = 1;
+  // main-step slots: two groups balanced by points (greedy in slot order)
+  int nmain = 0;
+  for (int s = 0; s < P->max_slots; ++s) {
+    const SlotHost &h = P->hs[s];
+    if (h.used && h.step <= h.nt - 1 && !(h.needs_ss2 && h.step == 1)) ++nmain;
+  }
+  P->split = P->split_on && nmain >= 2;
+  int64_t load[2] = {0, 0};
   for (int s = 0; s < P->max_slots; ++s) {
     SlotHost &h = P->hs[s];
     SlotDesc &d = P->sd[s];
     d.active = h.used && h.step <= h.nt - 1;
     if (!d.active) continue;
-    TileSet &T = (h.needs_ss2 && h.step == 1) ? P->first : P->main;
+    const bool first = h.needs_ss2 && h.step == 1;
+    int g = 0;
+    if (!first && P->split) {
+      g = load[1] < load[0] ? 1 : 0;
+      load[g] += h.npad;
+    }
+    TileSet &T = first ? P->first : (g ? P->main2 : P->main);
     d.tile_begin = (int)T.tiles.size();
     slot_tiles(P, s, d, T.tiles);
     d.tile_count = (int)T.tiles.size() - d.tile_begin;
@@ -629,7 +655,7 @@ int rebuild_tables(nls_pool *P) {
   int rb = 1;
   while (rb * 256 * 4 < max_ring && rb < 256) rb *= 2;
   P->ring_blocks = rb;
-  for (TileSet *T : {&P->main, &P->first}) {
+  for (TileSet *T : {&P->main, &P->main2, &P->first}) {
     T->live = (int)T->tiles.size();
     T->nlist = (int)T->list.size();
     int rc = ensure_tiles(P, *T, std::max(T->live, 1));
@@ -696,8 +722,8 @@ int rebuild_tables(nls_pool *P) {
     if (T->nlist) CK(cudaMemcpyAsync(T->d_list, T->list.data(), sizeof(int) * T->nlist, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlist, &T->nlist, sizeof(int), cudaMemcpyHostToDevice, P->stream));
   }
-  int rc = ensure_partials(P, std::max(std::max(P->main.lcap, P->first.lcap),
-                                       std::max(P->main.tcap, P->first.tcap)));
+  int rc = ensure_partials(P, std::max({P->main.lcap, P->main2.lcap, P->first.lcap, P->main.tcap,
+                                        P->main2.tcap, P->first.tcap}));
   if (rc) return rc;
   CK(cudaMemcpyAsync(P->d_slots, P->sd.data(), sizeof(SlotDesc) * P->max_slots, cudaMemcpyHostToDevice, P->stream));
   // the pageable sources above are staged by the runtime before returning;
@@ -706,7 +732,7 @@ int rebuild_tables(nls_pool *P) {
   return NLS_OK;
 }
 
-StepArgs base_args(const nls_pool *P, const TileSet &T) {
+StepArgs base_args(const nls_pool *P, const TileSet &T, int group = 0) {
   StepArgs a;
   std::memset(&a, 0, sizeof(a));
   a.slots = P->d_slots;
@@ -730,8 +756,8 @@ StepArgs base_args(const nls_pool *P, const TileSet &T) {
   a.vstride = P->cap;
   a.k = P->k;
   a.kv = P->k - 1;
-  a.part = P->part;
   a.part_stride = (long long)P->part_tiles * 2 * (P->cplx ? 9 : 6);
+  a.part = P->part + (group ? (long long)std::max(P->k - 1, 1) * a.part_stride : 0);
   a.scal = P->d_scal;
   a.beta0 = P->d_beta0;
   a.coef = P->d_coef;
@@ -743,16 +769,16 @@ StepArgs base_args(const nls_pool *P, const TileSet &T) {
 }
 
 // One Krylov application family (first pass, Lanczos passes, f(T), final).
-int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &nk) {
+int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &nk, cudaStream_t st) {
   const int grid = T.cap, hc = P->step_hc;
   if (L.first_lt[hc]) {
     StepArgs f = a;
     f.tiles = T.d_lt;
     f.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
     f.lt_stride = T.d_nlt1;
-    CK(L.first[hc](f, T.lcap, P->stream));
+    CK(L.first[hc](f, T.lcap, st));
   } else {
-    CK(L.first[hc](a, grid, P->stream));
+    CK(L.first[hc](a, grid, st));
   }
   ++nk;
   StepArgs b = a;  // 2-D passes: one warp per (strip, sequence) or one TMA block per tile
@@ -772,24 +798,24 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
   }
   for (int j = 1; j <= P->k - 2; ++j) {
     b.j = j;
-    CK(lf(b, lgrid, P->stream));
+    CK(lf(b, lgrid, st));
     ++nk;
   }
-  CK(P->ks.ftri(a, P->max_slots, P->stream));
+  CK(P->ks.ftri(a, P->max_slots, st));
   ++nk;
-  CK(L.final_[hc](a, grid, P->stream));
+  CK(L.final_[hc](a, grid, st));
   ++nk;
   return NLS_OK;
 }
 
 // The launch sequence of one step over tile set T. mode_first: SEWI Strang step.
-int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
+int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first, cudaStream_t st, int group = 0) {
   int nk = 0;
-  StepArgs a = base_args(P, T);
+  StepArgs a = base_args(P, T, group);
   const int m = P->method;
   if (is_sv(m)) {
     a.sv_pingpong = 1;
-    CK(P->ks.sv[P->step_hc](a, T.cap, P->stream));
+    CK(P->ks.sv[P->step_hc](a, T.cap, st));
     ++nk;
   } else if (m == NLS_KG_GAUTSCHI || m == NLS_SP4_GAUTSCHI) {
     // kg_single.cuh:103-111: cos(tau sqrt A) u and sinc^2(tau sqrt A) g(u), A = -L
@@ -801,7 +827,7 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
     a.incr[1] = 0;
     a.tsc[0][0] = 1.0;
     a.tsc[1][0] = 1.0;
-    int rc = run_krylov(P, T, P->ks.kg, a, nk);
+    int rc = run_krylov(P, T, P->ks.kg, a, nk, st);
     if (rc) return rc;
   } else if (m == NLS_NLSE_SS2 || mode_first) {
     // nlse_dev.hpp:190: exp(i dt L) with dti = (0, dt)
@@ -810,7 +836,7 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
     a.fkind[0] = FK_EXP;
     a.incr[0] = 1;
     a.tsc[0][1] = 1.0;
-    int rc = run_krylov(P, T, P->ks.ss2, a, nk);
+    int rc = run_krylov(P, T, P->ks.ss2, a, nk, st);
     if (rc) return rc;
   } else {
     // nlse_dev.hpp:219-223: sinc(dt L) B(u) and exp(2 i dt L) u_prev, then exp(i dt L) y_a
@@ -822,38 +848,58 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first) {
     a.incr[1] = 1;
     a.tsc[0][0] = 1.0;
     a.tsc[1][1] = 2.0;
-    int rc = run_krylov(P, T, P->ks.sewi_a, a, nk);
+    int rc = run_krylov(P, T, P->ks.sewi_a, a, nk, st);
     if (rc) return rc;
-    StepArgs b = base_args(P, T);
+    StepArgs b = base_args(P, T, group);
     b.nseq = 1;
     b.op_sign = 1.0;
     b.fkind[0] = FK_EXP;
     b.incr[0] = 0;
     b.tsc[0][1] = 1.0;
-    rc = run_krylov(P, T, P->ks.sewi_b, b, nk);
+    rc = run_krylov(P, T, P->ks.sewi_b, b, nk, st);
     if (rc) return rc;
   }
   a.sv_pingpong = is_sv(m) ? 1 : 0;
-  CK(P->ks.ring(a, P->ring_blocks, P->max_slots, P->stream));
+  CK(P->ks.ring(a, P->ring_blocks, P->max_slots, st));
   ++nk;
-  CK(launch_advance(a, P->max_slots, P->stream));
+  CK(launch_advance(a, P->max_slots, st));
   ++nk;
   P->kernels_per_step = nk;
   return NLS_OK;
 }
 
+// The main step: one launch sequence, or (two groups) a fork onto stream2, the
+// two groups' sequences side by side, and a join back onto the pool stream.
+int enqueue_main(nls_pool *P) {
+  if (!P->split) return enqueue_step(P, P->main, false, P->stream, 0);
+  CK(cudaEventRecord(P->ev_fork, P->stream));
+  CK(cudaStreamWaitEvent(P->stream2, P->ev_fork, 0));
+  int rc = enqueue_step(P, P->main, false, P->stream, 0);
+  if (rc) return rc;
+  const int nk0 = P->kernels_per_step;
+  rc = enqueue_step(P, P->main2, false, P->stream2, 1);
+  if (rc) return rc;
+  P->kernels_per_step += nk0;
+  CK(cudaEventRecord(P->ev_join, P->stream2));
+  CK(cudaStreamWaitEvent(P->stream, P->ev_join, 0));
+  return NLS_OK;
+}
+
 int run_main_step(nls_pool *P) {
-  if (!P->use_graph) return enqueue_step(P, P->main, false);
+  if (!P->use_graph) return enqueue_main(P);
+  const int sp = P->split ? 1 : 0;
   if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks ||
       P->graph_hc != P->step_hc || P->graph_part != (void *)P->part ||
-      P->graph_lcap != P->main.lcap || P->graph_tcap != P->main.tcap) {
+      P->graph_lcap != P->main.lcap || P->graph_tcap != P->main.tcap || P->graph_split != sp ||
+      (sp && (P->graph_tiles2 != P->main2.cap || P->graph_lcap2 != P->main2.lcap ||
+              P->graph_tcap2 != P->main2.tcap))) {
     if (P->gexec) {
       cudaGraphExecDestroy(P->gexec);
       P->gexec = nullptr;
     }
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(P, P->main, false);
+    int rc = enqueue_main(P);
     cudaError_t e2 = cudaStreamEndCapture(P->stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
@@ -869,6 +915,10 @@ int run_main_step(nls_pool *P) {
     P->graph_part = (void *)P->part;
     P->graph_lcap = P->main.lcap;
     P->graph_tcap = P->main.tcap;
+    P->graph_split = sp;
+    P->graph_tiles2 = P->main2.cap;
+    P->graph_lcap2 = P->main2.lcap;
+    P->graph_tcap2 = P->main2.tcap;
   }
   CK(cudaGraphLaunch(P->gexec, P->stream));
   return NLS_OK;
@@ -952,13 +1002,13 @@ int pool_step_once(nls_pool *P) {
   int rc0 = pool_step_prepare(P);
   if (rc0) return rc0;
   if (P->main.nlist == 0 && P->first.nlist == 0) return NLS_OK;
-  for (TileSet *T : {&P->first, &P->main})
+  for (TileSet *T : {&P->first, &P->main, &P->main2})
     for (int s : T->list) {
       int rc = wait_frame(P, P->hs[s], P->hs[s].step);
       if (rc) return rc;
     }
   if (P->first.nlist) {
-    int rc = enqueue_step(P, P->first, true);
+    int rc = enqueue_step(P, P->first, true, P->stream, 0);
     if (rc) return rc;
   }
   if (P->main.nlist) {
@@ -967,7 +1017,7 @@ int pool_step_once(nls_pool *P) {
   }
   CK(cudaEventRecord(P->ev_step, P->stream));
   CK(cudaStreamWaitEvent(P->copy_stream, P->ev_step, 0));
-  for (TileSet *T : {&P->first, &P->main})
+  for (TileSet *T : {&P->first, &P->main, &P->main2})
     for (int s : T->list) {
       SlotHost &h = P->hs[s];
       int rc = issue_copies(P, h, P->sd[s], h.step);
@@ -1170,7 +1220,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_diag_part, sizeof(double) * max_slots * DIAG_BLOCKS * 4);
   if (!rc) rc = al((void **)&P->d_diag_out, sizeof(double) * max_slots * 4);
   if (!rc) rc = al((void **)&P->d_diag_ticket, sizeof(int) * max_slots);
-  for (TileSet *T : {&P->main, &P->first}) {
+  for (TileSet *T : {&P->main, &P->main2, &P->first}) {
     if (!rc) rc = al((void **)&T->d_ntt1, sizeof(int));
     if (!rc) rc = al((void **)&T->d_ntt2, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlt1, sizeof(int));
@@ -1186,6 +1236,13 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc && cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "stream");
   if (!rc && cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "stream");
   if (!rc && cudaEventCreateWithFlags(&P->ev_step, cudaEventDisableTiming) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "event");
+  if (!rc && cudaStreamCreateWithFlags(&P->stream2, cudaStreamNonBlocking) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "stream");
+  if (!rc && cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "event");
+  if (!rc && cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming) != cudaSuccess) rc = fail(NLS_ERR_CUDA, "event");
+  if (!rc) {
+    const char *e = std::getenv("NLS_SPLIT");
+    P->split_on = !(e && std::atoi(e) == 0);
+  }
   if (!rc) {
     cudaError_t e = cudaMemsetAsync(P->d_state, 0, sizeof(SlotState) * max_slots, P->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->snap, 0, sizeof(double) * ce * 2 * NF, P->stream);
@@ -1201,6 +1258,9 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
     if (P->stream) cudaStreamDestroy(P->stream);
     if (P->copy_stream) cudaStreamDestroy(P->copy_stream);
     if (P->ev_step) cudaEventDestroy(P->ev_step);
+    if (P->stream2) cudaStreamDestroy(P->stream2);
+    if (P->ev_fork) cudaEventDestroy(P->ev_fork);
+    if (P->ev_join) cudaEventDestroy(P->ev_join);
     delete P;
     return rc;
   }
@@ -1449,32 +1509,59 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
     if (rc) return rc;
   }
   if (P->main.nlist == 0) return fail(NLS_ERR_STATE, "no active slot");
-  StepArgs a = base_args(P, P->main);
-  a.j = j;
-  a.op_sign = P->cplx ? 1.0 : -1.0;
   const Launch &L = P->cplx ? (P->method == NLS_NLSE_SS2 ? P->ks.ss2 : P->ks.sewi_a) : P->ks.kg;
-  a.nseq = P->method == NLS_NLSE_SS2 ? 1 : 2;
+  const int hc = P->step_hc;
+  // pass j over every main-step group, launched as the step launches it (the
+  // two groups side by side on the pool stream and stream2)
+  StepArgs args[2];
+  int grids[2];
+  LaunchFn fns[2];
+  const int ng = P->split ? 2 : 1;
+  for (int g = 0; g < ng; ++g) {
+    const TileSet &T = g ? P->main2 : P->main;
+    StepArgs a = base_args(P, T, g);
+    a.j = j;
+    a.op_sign = P->cplx ? 1.0 : -1.0;
+    a.nseq = P->method == NLS_NLSE_SS2 ? 1 : 2;
+    int grid = T.cap;
+    LaunchFn lf = L.lanczos[hc];
+    if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
+      a.tiles = T.d_tt;
+      a.ntiles = a.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
+      a.lt_stride = T.d_ntt1;
+      grid = T.tcap;
+      lf = P->ks.lanczos_tma;
+    } else if (P->dim == 2) {
+      a.tiles = T.d_lt;
+      a.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
+      a.lt_stride = T.d_nlt1;
+      grid = T.lcap;
+    }
+    args[g] = a;
+    grids[g] = grid;
+    fns[g] = lf;
+  }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int hc = P->step_hc;
-  int grid = P->main.cap;
-  LaunchFn lf = L.lanczos[hc];
-  if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
-    a.tiles = P->main.d_tt;
-    a.ntiles = a.nseq == 2 ? P->main.d_ntt2 : P->main.d_ntt1;
-    a.lt_stride = P->main.d_ntt1;
-    grid = P->main.tcap;
-    lf = P->ks.lanczos_tma;
-  } else if (P->dim == 2) {
-    a.tiles = P->main.d_lt;
-    a.ntiles = a.nseq == 2 ? P->main.d_nlt2 : P->main.d_nlt1;
-    a.lt_stride = P->main.d_nlt1;
-    grid = P->main.lcap;
-  }
-  CK(lf(a, grid, P->stream));  // warm
+  auto once = [&]() -> int {
+    if (ng == 1) {
+      CK(fns[0](args[0], grids[0], P->stream));
+      return NLS_OK;
+    }
+    CK(cudaEventRecord(P->ev_fork, P->stream));
+    CK(cudaStreamWaitEvent(P->stream2, P->ev_fork, 0));
+    CK(fns[0](args[0], grids[0], P->stream));
+    CK(fns[1](args[1], grids[1], P->stream2));
+    CK(cudaEventRecord(P->ev_join, P->stream2));
+    CK(cudaStreamWaitEvent(P->stream, P->ev_join, 0));
+    return NLS_OK;
+  };
+  int rc = once();  // warm
+  if (rc) return rc;
   CK(cudaEventRecord(e0, P->stream));
-  for (int i = 0; i < iters; ++i) CK(lf(a, grid, P->stream));
+  for (int i = 0; i < iters && !rc; ++i) rc = once();
+  if (rc) return rc;
   CK(cudaEventRecord(e1, P->stream));
   CK(cudaEventSynchronize(e1));
   float t = 0.f;
@@ -1485,6 +1572,7 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
   if (points) {
     int64_t pts = 0;
     for (int s : P->main.list) pts += P->hs[s].n;
+    for (int s : P->main2.list) pts += P->hs[s].n;
     *points = pts;
   }
   return NLS_OK;
@@ -1505,7 +1593,10 @@ int nls_pool_destroy(nls_pool *P) {
   pool_free_device(P);
   cudaStreamDestroy(P->stream);
   cudaStreamDestroy(P->copy_stream);
+  cudaStreamDestroy(P->stream2);
   cudaEventDestroy(P->ev_step);
+  cudaEventDestroy(P->ev_fork);
+  cudaEventDestroy(P->ev_join);
   delete P;
   return NLS_OK;
 }
