@@ -64,49 +64,83 @@ def pass_bytes_per_gp(s=4):
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
-
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, power and clock-event reasons of this rank's GPU, read through
+    NVML (read-only queries) every 2 ms while the timed region runs. The GPU is
+    found by the CUDA device's PCI bus id, so the sample is of the device the
+    kernels run on whatever CUDA_VISIBLE_DEVICES maps."""
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
         self._stop = threading.Event()
         self._t = None
+        self._h = None
+        self.device = None
+
+    def _handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            self.device = bus
+            return N.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip().isdigit()]
+            idx = int(ids[self.index]) if self.index < len(ids) else self.index
+            self.device = f"nvml index {idx}"
+            return N.nvmlDeviceGetHandleByIndex(idx)
+
+    def _sample(self):
+        import pynvml as N
+        sm = N.nvmlDeviceGetClockInfo(self._h, N.NVML_CLOCK_SM)
+        mx = N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM)
+        rs = N.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        self.rows.append((sm, mx, rs))
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
+                self._sample()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.002)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._h = self._handle()
+            self._sample()
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._h = None
         return self
 
     def __exit__(self, *a):
         self._stop.set()
-        self._t.join(timeout=10)
+        if self._t:
+            self._t.join(timeout=10)
+        if self._h is not None:
+            try:
+                self._sample()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4)
-                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+        import pynvml as N
+        names = {N.nvmlClocksEventReasonHwSlowdown: "hw_slowdown",
+                 N.nvmlClocksEventReasonHwThermalSlowdown: "hw_thermal_slowdown",
+                 N.nvmlClocksEventReasonSwThermalSlowdown: "sw_thermal_slowdown",
+                 N.nvmlClocksEventReasonSwPowerCap: "sw_power_cap",
+                 N.nvmlClocksEventReasonHwPowerBrakeSlowdown: "hw_power_brake_slowdown"}
+        reasons = sorted({nm for _, _, rs in self.rows for bit, nm in names.items() if rs & bit})
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows),
+                "sm_max_mhz": max(r[1] for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows), "source": f"NVML every 2 ms ({self.device})"}
 
 
 def make_batch(B, rank, k, nt=None, ns=None, T=None):
@@ -368,7 +402,7 @@ def run_ours(args, ws, rank, lrank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
