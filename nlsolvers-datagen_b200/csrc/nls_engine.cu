@@ -89,6 +89,7 @@ struct Launch {
   LaunchFn lanczos[2] = {nullptr, nullptr};
   LaunchFn final_[2] = {nullptr, nullptr};
   bool first_lt[2] = {false, false};  // the first pass runs on the pass tile table
+  LaunchFn lanczos_lo[2] = {nullptr, nullptr};  // pass j = 1 with the low word of u (cosine sequence)
 };
 
 template <typename E, int SRC, bool HC>
@@ -142,6 +143,10 @@ cudaError_t launch2_lanczos1_f32c(const StepArgs &a, int tiles, cudaStream_t st)
     k2_lanczos1_f32c<5><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   else
     k2_lanczos1_f32c<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch2_lanczos1_f32c_lo(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_lanczos1_f32c<4, true><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch2_lanczos1_f32b(const StepArgs &a, int tiles, cudaStream_t st) {
@@ -317,6 +322,7 @@ template <typename R> KSet make_real2() {
       k.kg.first[0] = launch2_first_f32;
       k.kg.first_lt[0] = true;
     }
+    if (f32_pass_form() == 3) k.kg.lanczos_lo[0] = launch2_lanczos1_f32c_lo;
     k.lanczos_tma = launch2t_lanczos_f32;
     k.set_attrs = attrs_tma_f32;
   }
@@ -798,7 +804,9 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
   }
   for (int j = 1; j <= P->k - 2; ++j) {
     b.j = j;
-    CK(lf(b, lgrid, st));
+    LaunchFn fj = lf;
+    if (j == 1 && lf == L.lanczos[hc] && L.lanczos_lo[hc]) fj = L.lanczos_lo[hc];
+    CK(fj(b, lgrid, st));
     ++nk;
   }
   CK(P->ks.ftri(a, P->max_slots, st));

@@ -1505,18 +1505,27 @@ __device__ __forceinline__ F4 lds16(uint32_t saddr) {
   return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
 }
 
-template <bool EDGE>
+// LO (pass j = 1 only): the warps of the cosine sequence, whose start vector
+// V_0 is the high word of u, stream the low word u_lo through ring B (unused
+// at j = 1) and add its stencil and alpha terms when forming v_1, so v_1 is
+// formed from u to about twice FP32 precision. The reference's truncated
+// Lanczos matrix (T[k-1,k-1] = 0) makes the result sensitive to the
+// high-frequency rounding noise of the start vector under the stencil; later
+// vectors can be rounded to FP32 without effect.
+template <bool EDGE, bool LO = false>
 __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB, const float *safe, float *pJ, int P,
                                                 int r0, int r1, int ny, bool ld, bool io, bool hasB, float2 CA,
                                                 float2 CB, const F4 &CSx, const F4 &OPx, const F4 &xmiss,
-                                                double *acc, uint32_t cellA, uint32_t cellB) {
+                                                double *acc, uint32_t cellA, uint32_t cellB, bool lo = false) {
+  const bool bl = LO && lo;  // ring B carries the low word of V_0
   // fetch f: A row r0-2+f into slot f % CPD of ring A, B row r0-2+f into ring B
   // (fetch 0 of B is never read); one commit group per fetch
   auto fetch = [&](int f) {
     const int r = r0 - 2 + f;
     const uint32_t off = (uint32_t)((f % CPD) * 512);
     const bool okA = EDGE ? (ld && r >= 0 && r < ny && r <= r1 + 1) : (ld && r <= r1 + 1);
-    const bool okB = EDGE ? (ld && hasB && f >= 1 && r >= 0 && r < ny && r <= r1) : (ld && hasB && f >= 1 && r <= r1);
+    const bool okB = bl ? okA
+                        : EDGE ? (ld && hasB && f >= 1 && r >= 0 && r < ny && r <= r1) : (ld && hasB && f >= 1 && r <= r1);
     cp16z(cellA + off, okA ? (const void *)(pA + r * P) : (const void *)safe, okA);
     cp16z(cellB + off, okB ? (const void *)(pB + r * P) : (const void *)safe, okB);
     cp_async_commit();
@@ -1526,15 +1535,16 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
   // skipped (the test is warp-uniform), so those slots keep stale rows that
   // only discarded iterations read
   const float *gA = ld ? pA + (r0 - 2) * P : safe;
-  const float *gB = (ld && hasB) ? pB + (r0 - 2) * P : safe;
-  const int stA = ld ? P : 0, stB = (ld && hasB) ? P : 0;
-  const int szA = ld ? 16 : 0, szB = (ld && hasB) ? 16 : 0;
-  const int fA_last = r1 + 3 - r0, fB_last = r1 + 2 - r0;
+  const bool useB = ld && (hasB || bl);
+  const float *gB = useB ? pB + (r0 - 2) * P : safe;
+  const int stA = ld ? P : 0, stB = useB ? P : 0;
+  const int szA = ld ? 16 : 0, szB = useB ? 16 : 0;
+  const int fA_last = r1 + 3 - r0, fB_last = bl ? fA_last : r1 + 2 - r0, fB_first = bl ? 0 : 1;
   constexpr uint32_t RM = CPD * 512 - 1;
   uint32_t soff = 0, ldA = 2 * 512, ldB = 512;
   auto fetch_fast = [&](int f) {
     if (f <= fA_last) cp16s(cellA + soff, gA, szA);
-    if (f >= 1 && f <= fB_last) cp16s(cellB + soff, gB, szB);
+    if (f >= fB_first && f <= fB_last) cp16s(cellB + soff, gB, szB);
     gA += stA;
     gB += stB;
     soff = (soff + 512) & RM;
@@ -1548,16 +1558,22 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
   cp_async_wait<CPD - 2>();
   F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2;
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
-  F4 V0 = zero4, V1 = zero4, V2 = zero4, Bq;
+  F4 V0 = zero4, V1 = zero4, V2 = zero4, Bq = zero4;
+  F4 L0 = zero4, L1 = zero4, L2 = zero4;  // low word of V_0 (LO)
+  if (LO && bl) {
+    L0 = lds16(cellB);
+    L1 = lds16(cellB + 512);
+  }
   float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f), q5 = f2(0.f);
   const int qb = r0 - 1;
   const int nit = ((r1 - qb + 1) + 2) / 3 * 3;
-#define NLSB_ROW3(Am, Ac, Ap, Vm, Vc, Vn)                                                       \
+#define NLSB_ROW3(Am, Ac, Ap, Lm, Lc, Lp, Vm, Vc, Vn)                                           \
   {                                                                                           \
     const int q = qb + it;                                                                    \
     cp_async_wait<CPD - 3>();                                                                 \
     Ap = lds16(cellA + ldA);                                                                  \
-    Bq = lds16(cellB + ldB);                                                                  \
+    if (LO && bl) Lp = lds16(cellB + ldA);                                                    \
+    else Bq = lds16(cellB + ldB);                                                             \
     ldA = (ldA + 512) & RM;                                                                   \
     ldB = (ldB + 512) & RM;                                                                   \
     if (EDGE) fetch(it + CPD);                                                                \
@@ -1573,6 +1589,13 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
       const F4 w = lap4(Am, Ac, Ap, lft, rgt, miss);                                          \
       Vn.a = fma2(CB, Bq.a, fma2(CA, Ac.a, mul2(CSx.a, w.a)));                                \
       Vn.b = fma2(CB, Bq.b, fma2(CA, Ac.b, mul2(CSx.b, w.b)));                                \
+      if (LO && bl) {                                                                         \
+        const float lftL = __shfl_up_sync(0xffffffffu, Lc.b.y, 1);                            \
+        const float rgtL = __shfl_down_sync(0xffffffffu, Lc.a.x, 1);                          \
+        const F4 wl = lap4(Lm, Lc, Lp, lftL, rgtL, miss);                                     \
+        Vn.a = add2(Vn.a, fma2(CA, Lc.a, mul2(CSx.a, wl.a)));                                 \
+        Vn.b = add2(Vn.b, fma2(CA, Lc.b, mul2(CSx.b, wl.b)));                                 \
+      }                                                                                       \
       if (EDGE) {                                                                             \
         const float2 rv = f2((q >= 0 && q < ny) ? 1.f : 0.f);                                 \
         Vn.a = mul2(Vn.a, rv);                                                                \
@@ -1604,9 +1627,9 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
   }
   for (int it0 = 0; it0 < nit; it0 += 3) {
     int it = it0;
-    NLSB_ROW3(A0, A1, A2, V1, V2, V0) ++it;
-    NLSB_ROW3(A1, A2, A0, V2, V0, V1) ++it;
-    NLSB_ROW3(A2, A0, A1, V0, V1, V2)
+    NLSB_ROW3(A0, A1, A2, L0, L1, L2, V1, V2, V0) ++it;
+    NLSB_ROW3(A1, A2, A0, L1, L2, L0, V2, V0, V1) ++it;
+    NLSB_ROW3(A2, A0, A1, L2, L0, L1, V0, V1, V2)
     acc[0] += (double)(q0.x + q0.y);
     acc[1] += (double)(q1.x + q1.y);
     acc[2] += (double)(q2.x + q2.y);
@@ -1619,7 +1642,7 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
   cp_async_wait<0>();
 }
 
-template <int MINB>
+template <int MINB, bool LO = false>
 __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
   using E = float;
   __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
@@ -1637,7 +1660,10 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
   const float *base = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
   const long long lane_off = s.off + S.col0;
   const float *pA = (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
-  const float *pB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
+  // LO at j = 1: the cosine sequence (0) streams u_lo as ring B (V_0 = u_hi there)
+  const bool lo = LO && sq == 0;
+  const float *pB = lo ? (const float *)a.f.u_lo + lane_off
+                       : (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
   float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
   F4 CSx, OPx, xmiss;
   {
@@ -1659,9 +1685,11 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
   const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   if (r0 >= 2 && r1 <= ny - 2)
-    lz1f32_cp_march<false>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA, cellB);
+    lz1f32_cp_march<false, LO>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA,
+                               cellB, lo);
   else
-    lz1f32_cp_march<true>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA, cellB);
+    lz1f32_cp_march<true, LO>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA,
+                              cellB, lo);
   acc[0] *= sA;
   acc[2] *= sA;
   acc[5] *= sA * sA;

@@ -547,6 +547,15 @@ int run_nlse(const orc_problem *p, const Derived &D, const cd *u0, const double 
 
 extern "C" {
 
+// Ghost copies alone (apply_bc) on a real or interleaved complex field.
+void orc_apply_bc(int32_t dim, int32_t nx, int32_t ny, int32_t nz, double *u, int32_t cplx) {
+  Grid g{dim, nx, ny, dim == 3 ? nz : 1, (long)nx * ny * (dim == 3 ? nz : 1)};
+  if (cplx)
+    apply_bc(g, reinterpret_cast<std::complex<double> *>(u));
+  else
+    apply_bc(g, u);
+}
+
 void orc_apply_operator(int32_t dim, int32_t nx, int32_t ny, int32_t nz, double inv_h2,
                         double sign, const double *c, const double *x, double *y,
                         int32_t is_complex) {

@@ -61,6 +61,8 @@ typedef struct orc_problem {
 
 /* y = sign * L(c) x on the full grid; L is the no-flux finite-volume operator of
    laplacians.hpp:54-103 / 158-218 scaled by inv_h2. is_complex: x,y interleaved. */
+/* The Neumann ghost copies of device/include/boundaries.cuh:9-81, in place. */
+void orc_apply_bc(int32_t dim, int32_t nx, int32_t ny, int32_t nz, double *u, int32_t cplx);
 void orc_apply_operator(int32_t dim, int32_t nx, int32_t ny, int32_t nz,
                         double inv_h2, double sign, const double *c,
                         const double *x, double *y, int32_t is_complex);

@@ -70,6 +70,8 @@ def lib():
         L.orc_run.argtypes = [ctypes.POINTER(_Problem), dp, dp, dp, dp, dp, dp]
         L.orc_run.restype = ctypes.c_int32
         L.orc_num_threads.restype = ctypes.c_int32
+        L.orc_apply_bc.argtypes = [ctypes.c_int32] * 4 + [dp, ctypes.c_int32]
+        L.orc_apply_bc.restype = None
         L.orc_real_begin.argtypes = [ctypes.POINTER(_Problem), dp, dp, dp, dp]
         L.orc_real_begin.restype = ctypes.c_void_p
         L.orc_real_advance.argtypes = [ctypes.c_void_p, ctypes.c_int32, dp]
@@ -146,6 +148,15 @@ def matfunc(x, c, dim, inv_h2, sign, k, ftype, t, reorth=True):
     if rc != 0:
         raise RuntimeError(f"matfunc failed: {rc}")
     return y, Tm.reshape(k, k).T
+
+
+def apply_bc(u, dim):
+    """The reference's ghost copies on a copy of u ((ny, nx) or (nz, ny, nx))."""
+    cplx = np.iscomplexobj(u)
+    u = _f64(u, cplx).copy()
+    nz, ny, nx = (u.shape if dim == 3 else (1,) + u.shape)
+    lib().orc_apply_bc(dim, nx, ny, nz, _p(u.view(np.float64)), int(cplx))
+    return u
 
 
 def philox_normal(seed, step, point):

@@ -212,3 +212,55 @@ def test_diagnostics_restatement_matches_reference_functions():
         nx, ny, Lx, Ly = g[f"nlse{i}_geom"]
         got = D.nlse(g[f"nlse{i}_u"], (Ly, Lx))
         np.testing.assert_allclose(got, g[f"nlse{i}_diag"], rtol=1e-13, atol=1e-300)
+
+
+def _reference_bc_copies(u):
+    """The reference's ghost copies replayed literally on a flat buffer, in its
+    order and with its index convention (device/include/boundaries.cuh:9-19:
+    element (i, j) at i*ny + j; :23-81: (x, y, z) at (x*ny + y)*nz + z), for the
+    square / cubic grids its drivers accept."""
+    f = u.ravel().copy()
+    if u.ndim == 2:
+        nx = ny = u.shape[0]
+        f[0 * ny + 1:0 * ny + 1 + ny - 2] = f[1 * ny + 1:1 * ny + 1 + ny - 2]
+        f[(nx - 1) * ny + 1:(nx - 1) * ny + 1 + ny - 2] = f[(nx - 2) * ny + 1:(nx - 2) * ny + 1 + ny - 2]
+        for i in range(nx):
+            f[i * ny + 0] = f[i * ny + 1]
+        for i in range(nx):
+            f[i * ny + ny - 1] = f[i * ny + ny - 2]
+        return f.reshape(u.shape)
+    nx = ny = nz = u.shape[0]
+    at = lambda x, y, z: (x * ny + y) * nz + z  # noqa: E731
+    for y in range(1, ny - 1):      # x-min / x-max faces, interior y, z
+        for z in range(1, nz - 1):
+            f[at(0, y, z)] = f[at(1, y, z)]
+    for y in range(1, ny - 1):
+        for z in range(1, nz - 1):
+            f[at(nx - 1, y, z)] = f[at(nx - 2, y, z)]
+    for x in range(nx):              # y faces over all x, interior z
+        for z in range(1, nz - 1):
+            f[at(x, 0, z)] = f[at(x, 1, z)]
+    for x in range(nx):
+        for z in range(1, nz - 1):
+            f[at(x, ny - 1, z)] = f[at(x, ny - 2, z)]
+    for x in range(nx):              # z faces over all x, y
+        for y in range(ny):
+            f[at(x, y, 0)] = f[at(x, y, 1)]
+    for x in range(nx):
+        for y in range(ny):
+            f[at(x, y, nz - 1)] = f[at(x, y, nz - 2)]
+    return f.reshape(u.shape)
+
+
+@pytest.mark.parametrize("shape", [(4, 4), (5, 5), (4, 4, 4), (5, 5, 5)])
+def test_ghost_copies_corner_and_edge_order(oracle_mod, shape):
+    """Corners and edges come out of the reference's copy order; the oracle
+    replays it, and the result is the per-axis clamp to the interior."""
+    u = np.arange(1, np.prod(shape) + 1, dtype=np.float64).reshape(shape) * 1.5
+    got = oracle_mod.apply_bc(u, len(shape))
+    np.testing.assert_array_equal(got, _reference_bc_copies(u))
+    idx = np.meshgrid(*[np.clip(np.arange(n), 1, n - 2) for n in shape], indexing="ij")
+    np.testing.assert_array_equal(got, u[tuple(idx)])
+    uc = u + 1j * u[::-1]
+    gotc = oracle_mod.apply_bc(uc, len(shape))
+    np.testing.assert_array_equal(gotc, _reference_bc_copies(uc))
