@@ -266,6 +266,22 @@ def run_reference(args, ws, rank, budget_s=150.0):
     return 0
 
 
+def serving_leg(count=24, rate_hz=8.0, steps=(200, 600), seed=5):
+    """The serving mix (requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
+    64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D; Poisson arrivals), shortened
+    to `steps` per request so that it runs in seconds: latency percentiles
+    (arrival to last snapshot on the host) and aggregate throughput."""
+    from nlsb200 import serve
+    reqs = serve.mixed_requests(count, rate_hz, seed=seed, steps=steps)
+    srv = serve.Server(serve.default_classes(reqs, max_slots=16), chunk=10)
+    st = srv.run(reqs, timeout_s=300)
+    srv.close()
+    out = st.summary()
+    out.update({"requests": count, "rate_hz": rate_hz, "steps_per_request": list(steps),
+                "classes": sorted({r.cls for r in reqs}), "unit": UNIT})
+    return out
+
+
 def run_small(args, lrank):
     """--small: --batch trajectories (default 16) of the same workload (k=10,
     32-row segments), warmup + steps only; the case the ncu captures profile
@@ -401,6 +417,8 @@ def run_ours(args, ws, rank, lrank):
         "kernels_per_step": kernels,
         "clocks": clk.summary(),
     }
+    if ws == 1 and not args.no_serve:
+        line["serving"] = serving_leg()
     if ws == 1 and rank == 0 and not args.no_cpu:
         rate, steps, secs, cores = cpu_oracle_rate(cases)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
@@ -417,6 +435,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-mix leg")
     ap.add_argument("--small", action="store_true",
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
