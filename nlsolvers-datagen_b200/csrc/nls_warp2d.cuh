@@ -1167,14 +1167,17 @@ __device__ __forceinline__ float2 neg2(float2 x) { return make_float2(-x.x, -x.y
 
 // Row of the count-form operator (differences first): with zero-filled halo,
 // sum_nbr (v_nbr - v) + miss * v equals the masked sum over in-grid neighbours.
+// The x part (v_{e-1} - v_e) + (v_{e+1} - v_e) is formed from the five
+// differences b_e = v_{e+1} - v_e of the row (left difference = -b_{e-1}
+// exactly), so each difference is computed once for its two elements; the
+// result is bitwise the same as summing the two differences of each element.
 __device__ __forceinline__ F4 lap4(const F4 &m, const F4 &o, const F4 &p, float lft, float rgt,
                                    const F4 &miss) {
   const float2 nc0 = neg2(o.a), nc1 = neg2(o.b);
-  // x-neighbours of elements (0,1): (lft, o0) and (o1, o2); of (2,3): (o1, o2) / (o3, rgt)
-  const float2 xl0 = make_float2(lft, o.a.x), xr0 = make_float2(o.a.y, o.b.x);
-  const float2 xl1 = make_float2(o.a.y, o.b.x), xr1 = make_float2(o.b.y, rgt);
-  float2 s0 = add2(add2(xl0, nc0), add2(xr0, nc0));
-  float2 s1 = add2(add2(xl1, nc1), add2(xr1, nc1));
+  const float bm = __fsub_rn(o.a.x, lft), b0 = __fsub_rn(o.a.y, o.a.x), b1 = __fsub_rn(o.b.x, o.a.y),
+              b2 = __fsub_rn(o.b.y, o.b.x), b3 = __fsub_rn(rgt, o.b.y);
+  float2 s0 = make_float2(__fsub_rn(b0, bm), __fsub_rn(b1, b0));
+  float2 s1 = make_float2(__fsub_rn(b2, b1), __fsub_rn(b3, b2));
   s0 = add2(s0, add2(add2(m.a, nc0), add2(p.a, nc0)));
   s1 = add2(s1, add2(add2(m.b, nc1), add2(p.b, nc1)));
   return F4{fma2(miss.a, o.a, s0), fma2(miss.b, o.b, s1)};
