@@ -101,6 +101,7 @@ __device__ inline LzScal lz_from_dots(const double *t, double eps) {
     N1 = t[3]; N2 = t[4]; N3 = t[5];
   }
   LzScal s;
+  s.n2 = N2;
   s.dr = D1r; s.di = D1i;
   // a = D2 - conj(d) D3
   s.ar = D2r - (s.dr * D3r + s.di * D3i);

@@ -48,6 +48,7 @@ struct LzScal {
   double dr, di;  // d_j = <A v_j, v_{j-1}>  (lower subdiagonal T[j, j-1])
   double b;       // ||w_j||  (b_{j+1})
   double inv_b;   // 1/b or 0 after breakdown
+  double n2;      // |v_j|^2 as the pass that produced these scalars summed it
 };
 
 // Coefficients of the final combination y = sum_j W_j V_j + Lam * (A V_{k-2}).

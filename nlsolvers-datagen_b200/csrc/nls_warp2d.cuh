@@ -1567,8 +1567,11 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
     L0 = lds16(cellB);
     L1 = lds16(cellB + 512);
   }
-  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f), q5 = f2(0.f);
+  // |v_{j-1}|^2 is not summed here: it is the previous pass's |v_j|^2 (LzScal::n2)
+  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
   const int qb = r0 - 1;
+  float *sp = pJ + qb * P;  // row q of V_j (stores for q in [r0, r1): it in [1, r1 - r0])
+  const int it_last = r1 - r0;
   const int nit = ((r1 - qb + 1) + 2) / 3 * 3;
 #define NLSB_ROW3(Am, Ac, Ap, Lm, Lc, Lp, Vm, Vc, Vn)                                           \
   {                                                                                           \
@@ -1604,7 +1607,8 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
         Vn.a = mul2(Vn.a, rv);                                                                \
         Vn.b = mul2(Vn.b, rv);                                                                \
       }                                                                                       \
-      if (io && q >= r0 && q < r1) f4_store(pJ + q * P, Vn);                                  \
+      if (io && it >= 1 && it <= it_last) f4_store(sp, Vn);                                   \
+      sp += P;                                                                                \
     }                                                                                         \
     {                                                                                         \
       const int r = q - 1;                                                                    \
@@ -1624,7 +1628,6 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
         q2 = fma2(Am.a, Vc.a, fma2(Am.b, Vc.b, q2));                                          \
         q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                              \
         q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
-        q5 = fma2(Am.a, Am.a, fma2(Am.b, Am.b, q5));                                          \
       }                                                                                       \
     }                                                                                         \
   }
@@ -1638,8 +1641,7 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
     acc[2] += (double)(q2.x + q2.y);
     acc[3] += (double)(q3.x + q3.y);
     acc[4] += (double)(q4.x + q4.y);
-    acc[5] += (double)(q5.x + q5.y);
-    q0 = q1 = q2 = q3 = q4 = q5 = f2(0.f);
+    q0 = q1 = q2 = q3 = q4 = f2(0.f);
   }
 #undef NLSB_ROW3
   cp_async_wait<0>();
@@ -1695,7 +1697,6 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
                               cellB, lo);
   acc[0] *= sA;
   acc[2] *= sA;
-  acc[5] *= sA * sA;
   constexpr int ND = 6;
   double vals[ND];
 #pragma unroll
@@ -1708,6 +1709,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
     double tv[ND];
 #pragma unroll
     for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    tv[5] = L.n2;  // |v_{j-1}|^2, summed by the previous pass in the same order
     if (lane == 0) {
       a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
       a.ticket[t.slot * 2 + sq] = 0;
