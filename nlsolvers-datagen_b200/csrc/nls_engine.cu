@@ -1472,9 +1472,14 @@ int nls_pool_sync(nls_pool *P) {
   // device-side status (eigensolver convergence)
   std::vector<SlotState> st(P->max_slots);
   CK(cudaMemcpy(st.data(), P->d_state, sizeof(SlotState) * P->max_slots, cudaMemcpyDeviceToHost));
-  for (int s = 0; s < P->max_slots; ++s)
-    if (P->hs[s].used && st[s].status != 0)
-      return fail(NLS_ERR_NUMERIC, "tridiagonal eigensolver did not converge for slot " + std::to_string(s));
+  for (int s = 0; s < P->max_slots; ++s) {
+    if (!P->hs[s].used || st[s].status == 0) continue;
+    if (st[s].status == -9)
+      return fail(NLS_ERR_NUMERIC, "slot " + std::to_string(s) + " diverged: non-finite Lanczos coefficients"
+                  " (with NLSE SEWI, the reference operand order, sewi_variant 0, grows without bound;"
+                  " variant 1 is the corrected order)");
+    return fail(NLS_ERR_NUMERIC, "tridiagonal eigensolver did not converge for slot " + std::to_string(s));
+  }
   return NLS_OK;
 }
 

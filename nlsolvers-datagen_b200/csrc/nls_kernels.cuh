@@ -691,7 +691,15 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
     F.beta0 = beta0;
     F.kv = k - 1;
     a.scal[(slot * 2 + sq) * KMAX + jl] = Lk;
-    if (status) a.state[slot].status = -8;
+    // non-finite Lanczos scalars: the trajectory itself diverged (-9), as
+    // opposed to a QL sweep that did not converge on finite data (-8)
+    bool finite = isfinite(beta0) && isfinite(Lk.b);
+    for (int jj = 0; jj < jl; ++jj) {
+      const LzScal &L = a.scal[(slot * 2 + sq) * KMAX + jj];
+      finite = finite && isfinite(L.ar) && isfinite(L.ai) && isfinite(L.dr) && isfinite(L.di) && isfinite(L.b);
+    }
+    if (!finite) a.state[slot].status = -9;
+    else if (status) a.state[slot].status = -8;
   }
 }
 
@@ -907,7 +915,15 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
     F.beta0 = beta0;
     F.kv = k - 1;
     a.scal[(slot * 2 + sq) * KMAX + jl] = Lk;
-    if (status) a.state[slot].status = -8;
+    // non-finite Lanczos scalars: the trajectory itself diverged (-9), as
+    // opposed to a QL sweep that did not converge on finite data (-8)
+    bool finite = isfinite(beta0) && isfinite(Lk.b);
+    for (int jj = 0; jj < jl; ++jj) {
+      const LzScal &L = a.scal[(slot * 2 + sq) * KMAX + jj];
+      finite = finite && isfinite(L.ar) && isfinite(L.ai) && isfinite(L.dr) && isfinite(L.di) && isfinite(L.b);
+    }
+    if (!finite) a.state[slot].status = -9;
+    else if (status) a.state[slot].status = -8;
   }
 }
 

@@ -107,3 +107,26 @@ def test_cfg2_size_batch_properties():
     sp, u0, v0, m, c = cases[17]
     otraj, _ = _oracle(sp, u0, v0, m, c)
     assert rel_l2(infos[17].traj, otraj) < TOL32
+
+
+def test_sewi_reference_order_diverges_and_is_reported():
+    """The reference's SEWI operand order (sewi_variant 0, nlse_dev.hpp:225-229)
+    grows without bound on these inputs (the FP64 oracle reaches |u| ~ 1e138 by
+    step 8 and then fails); the engine reports the divergence as
+    NLS_ERR_NUMERIC naming the corrected order, which runs cleanly."""
+    nl = _nl()
+    from nlsb200 import workloads as W
+    from nlsb200._lib import NlsError
+    spec, u0, _, m, c = W.nlse_case(64, 10.0, T=0.02, nt=20, ns=2, k=12, seed=0, precision=nl.FP32)
+    spec.method = nl.NLSE_SEWI
+    spec.sewi_variant = 0
+    with pytest.raises(NlsError) as err:
+        with nl.Solver(spec, u0, None, m) as s:
+            s.run()
+            s.snapshots()
+    assert err.value.code == -8 and "diverged" in str(err.value) and "variant 1" in str(err.value)
+    spec.sewi_variant = 1
+    with nl.Solver(spec, u0, None, m) as s:
+        s.run()
+        traj, _ = s.snapshots()
+    assert np.all(np.isfinite(traj)) and np.abs(traj).max() < 10
