@@ -769,7 +769,7 @@ StepArgs base_args(const nls_pool *P, const TileSet &T, int group = 0) {
   a.coef = P->d_coef;
   a.ticket = P->d_ticket;
   a.zeros = P->zeros;
-  a.scal_ready = P->dim == 2 ? 1 : 0;
+  a.scal_ready = 1;
   a.has_c = P->step_hc;
   return a;
 }

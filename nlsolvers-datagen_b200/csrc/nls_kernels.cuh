@@ -64,7 +64,7 @@ struct StepArgs {
   int *ticket;           // [slot][seq] arrival counters of the 2-D passes
   const int *lt_stride;  // device scalar: tiles per sequence section of the 2-D pass table
   const void *zeros;     // device buffer of zeros (source of out-of-grid rows)
-  int scal_ready;        // 1: every pass published its scalars (2-D path)
+  int scal_ready;        // 1: every pass published its scalars (f(T) reads them)
 };
 
 template <int DIM> struct Geo {
@@ -146,6 +146,45 @@ __device__ __forceinline__ void reduce_slot_partials(const double *part, int nv,
     for (int t = 0; t < tc; ++t) s += part[(long long)(tb + t) * nv + tid];
     tot[tid] = s;
   }
+}
+
+// Block-level publication (3-D passes): after this block stored its partials
+// of pass j at part_j + blockIdx.x * NV, the block that arrives last for its
+// slot sums the slot's partials in tile order (so the result does not depend
+// on which block came last) and publishes the Lanczos scalars of pass j (and
+// beta0 at j = 0); the next pass reads them instead of re-reducing.
+template <bool CP, typename R, int NSEQ, int NV>
+__device__ void publish_slot_scalars(const StepArgs &a, const SlotDesc &s, int slot, int j,
+                                     const double *part_j, double eps) {
+  constexpr int ND = CP ? 9 : 6;
+  __shared__ int last_s;
+  __shared__ double tot_s[NV];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last_s = atomicAdd(a.ticket + slot * 2, 1) == s.tile_count - 1;
+  __syncthreads();
+  if (!last_s) return;
+  __threadfence();
+  if (tid < NV) {
+    double acc = 0.0;
+    for (int t = 0; t < s.tile_count; ++t) acc += __ldcg(part_j + (long long)(s.tile_begin + t) * NV + tid);
+    tot_s[tid] = acc;
+  }
+  __syncthreads();
+  if (tid < NSEQ) {
+    const int sq = tid;
+    LzScal L;
+    if (j == 0) {
+      double b0;
+      L = lz_first<CP>(tot_s + sq * ND, eps, b0);
+      a.beta0[slot * 2 + sq] = b0;
+    } else {
+      L = lz_from_dots<CP>(tot_s + sq * ND, eps);
+    }
+    a.scal[(slot * 2 + sq) * KMAX + j] = L;
+  }
+  if (tid == 0) a.ticket[slot * 2] = 0;
 }
 
 template <typename R> struct Eps;
@@ -293,6 +332,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NT) k_first(StepArgs a) {
 #pragma unroll
   for (int q = 0; q < NV; ++q) vals[q] = acc[q].val();
   block_reduce_store<NV>(vals, red, a.part + (long long)blockIdx.x * NV);
+  publish_slot_scalars<Traits<E>::cplx, R, NSEQ, NV>(a, s, t.slot, 0, a.part, Eps<R>::v);
 }
 
 // --------------------------------------------------------- Lanczos pass j>=1
@@ -319,26 +359,19 @@ __global__ void __launch_bounds__(Geo<DIM>::NT) k_lanczos(StepArgs a) {
   __shared__ R cf_ib[NSEQ];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
 
-  // scalars of pass j-1 for this slot (redundantly per block, fixed order)
-  reduce_slot_partials(a.part + (long long)(j - 1) * a.part_stride, NV, s.tile_begin,
-                       s.tile_count, tot);
-  __syncthreads();
+  // scalars of pass j-1 for this slot, published by its last block
+  (void)tot;
   if (tid < NSEQ) {
     const int sq = tid;
-    LzScal L;
-    double b0;
+    const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+    const double b0 = a.beta0[t.slot * 2 + sq];
     double sA = 1.0, sB = 1.0;
     if (j == 1) {
-      L = lz_first<CP>(tot + sq * ND, Eps<R>::v, b0);
       sA = b0 > 0.0 ? 1.0 / b0 : 0.0;
       sB = 0.0;
-      if (t.local == 0) a.beta0[t.slot * 2 + sq] = b0;
-    } else {
-      L = lz_from_dots<CP>(tot + sq * ND, Eps<R>::v);
-      b0 = a.beta0[t.slot * 2 + sq];
-      if (j == 2) sB = b0 > 0.0 ? 1.0 / b0 : 0.0;
+    } else if (j == 2) {
+      sB = b0 > 0.0 ? 1.0 / b0 : 0.0;
     }
-    if (t.local == 0) a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)] = L;
     cf_s[sq][0] = R(sA);
     cf_s[sq][1] = R(sB);
     cf_s[sq][2] = R(L.ar);
@@ -457,6 +490,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NT) k_lanczos(StepArgs a) {
 #pragma unroll
   for (int q = 0; q < NV; ++q) vals[q] = acc[q].val();
   block_reduce_store<NV>(vals, red, a.part + (long long)j * a.part_stride + (long long)blockIdx.x * NV);
+  publish_slot_scalars<CP, R, NSEQ, NV>(a, s, t.slot, j, a.part + (long long)j * a.part_stride, Eps<R>::v);
 }
 
 // ------------------------------------------------------------ f(T) kernel
