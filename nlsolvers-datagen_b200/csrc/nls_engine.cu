@@ -489,7 +489,7 @@ struct nls_pool {
   std::vector<SlotHost> hs;
   std::vector<SlotDesc> sd;
   bool tables_dirty = true;
-  int seg2 = 32, seg3 = 16;
+  int seg2 = 32, seg3 = 32;  // march lengths (rows in 2-D, planes in 3-D)
   cudaStream_t stream = nullptr, copy_stream = nullptr, stream2 = nullptr;
   cudaEvent_t ev_step = nullptr, ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = true;
