@@ -779,8 +779,10 @@ template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
 // row costs one memory round trip; vectors past the first eight (k > 9) follow
 // in further batches. Coefficients sit in shared memory, one area per warp
 // (the warps of a block may belong to different slots).
+// Real FP32: built for four blocks per SM (128 registers; a few spill), which
+// measured faster than three blocks at 167 registers.
 template <typename E, int NSEQ, int FIN, bool HC>
-__global__ void __launch_bounds__(32 * WPB) k2_final(StepArgs a) {
+__global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 1) k2_final(StepArgs a) {
   using R = typename Traits<E>::R;
   using FR = FinRow<FIN, E>;
   constexpr int NB = 8;
