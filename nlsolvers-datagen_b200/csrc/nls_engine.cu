@@ -90,6 +90,7 @@ struct Launch {
   LaunchFn final_[2] = {nullptr, nullptr};
   bool first_lt[2] = {false, false};  // the first pass runs on the pass tile table
   LaunchFn lanczos_lo[2] = {nullptr, nullptr};  // pass j = 1 with the low word of u (cosine sequence)
+  bool lanczos_tt[2] = {false, false};  // 3-D passes run on the block table `tt`
 };
 
 template <typename E, int SRC, bool HC>
@@ -196,6 +197,20 @@ cudaError_t launch2_sv(const StepArgs &a, int tiles, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// 3-D FP32 warp-marching pass (one block per strip, band, segment and
+// sequence of the block table); NLS_K3=0 selects the shared-memory plane kernel.
+bool use_k3() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_K3");
+    return (e && std::atoi(e) == 0) ? 0 : 1;
+  }();
+  return v != 0;
+}
+cudaError_t launch3_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
+  k3_lanczos_f32<1><<<tiles, 32 * W3, sizeof(Smem3), st>>>(a);
+  return cudaGetLastError();
+}
+
 template <int DIM, typename E, int NSEQ, int SRC>
 cudaError_t launch_first(const StepArgs &a, int grid, cudaStream_t st) {
   k_first<DIM, E, NSEQ, SRC><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_first<DIM, E, NSEQ>(), st>>>(a);
@@ -259,6 +274,9 @@ struct KSet {
 
 template <int DIM, typename R> cudaError_t attrs_real() {
   cudaError_t e;
+  if constexpr (DIM == 3 && sizeof(R) == 4) {
+    if ((e = set_smem(k3_lanczos_f32<1>, sizeof(Smem3)))) return e;
+  }
   if ((e = set_smem(k_first<DIM, R, 2, SRC_KG>, smem_first<DIM, R, 2>()))) return e;
   if ((e = set_smem(k_lanczos<DIM, R, 2>, smem_lanczos<DIM, R, 2>()))) return e;
   if ((e = set_smem(k_final<DIM, R, 2, FIN_KG>, smem_final<DIM, R, 2>()))) return e;
@@ -284,6 +302,12 @@ template <typename R> KSet make_real3() {
   KSet k;
   k.kg.first[0] = k.kg.first[1] = launch_first<3, R, 2, SRC_KG>;
   k.kg.lanczos[0] = k.kg.lanczos[1] = launch_lanczos<3, R, 2>;
+  if constexpr (sizeof(R) == 4) {
+    if (use_k3()) {
+      k.kg.lanczos[0] = launch3_lanczos_f32;
+      k.kg.lanczos_tt[0] = true;
+    }
+  }
   k.kg.final_[0] = k.kg.final_[1] = launch_final<3, R, 2, FIN_KG>;
   k.sv[0] = k.sv[1] = launch_sv<3, R>;
   k.ftri = launch_ftri<R>;
@@ -684,24 +708,46 @@ int rebuild_tables(nls_pool *P) {
     if (T->live) CK(cudaMemcpyAsync(T->d_lt, T->lt.data(), sizeof(TileDesc) * n2, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlt1, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_nlt2, &T->lt_count2, sizeof(int), cudaMemcpyHostToDevice, P->stream));
-    if (P->dim == 2) {
+    {
       std::vector<TileDesc> base;
       for (int sidx : T->list) {
         SlotDesc &d = P->sd[sidx];
         d.tile_begin2 = (int)base.size();
-        const int nx4 = (d.nx + 3) / 4 * 4;
         int local = 0;
-        for (int p0 = 0; p0 < d.ny; p0 += P->seg2)
-          for (int x0 = 0; x0 < nx4; x0 += 512) {
-            TileDesc tq;
-            tq.slot = sidx;
-            tq.x0 = x0;
-            tq.y0 = std::min(512, nx4 - x0);
-            tq.p0 = p0;
-            tq.p1 = std::min(d.ny, p0 + P->seg2);
-            tq.local = 2 * local++;
-            base.push_back(tq);
-          }
+        if (P->dim == 2) {
+          // TMA pass tiles: <= 512 columns x segment rows
+          const int nx4 = (d.nx + 3) / 4 * 4;
+          for (int p0 = 0; p0 < d.ny; p0 += P->seg2)
+            for (int x0 = 0; x0 < nx4; x0 += 512) {
+              TileDesc tq;
+              tq.slot = sidx;
+              tq.x0 = x0;
+              tq.y0 = std::min(512, nx4 - x0);
+              tq.p0 = p0;
+              tq.p1 = std::min(d.ny, p0 + P->seg2);
+              tq.local = 2 * local++;
+              base.push_back(tq);
+            }
+        } else {
+          // 3-D pass blocks: strip (the 2-D strip split of the row's 16-byte
+          // vectors) x band of BY3 rows x segment planes; bands innermost, so
+          // blocks that share halo rows run side by side
+          const int nvec = (d.nx + 3) / 4;
+          const int nseg = (nvec + 29) / 30;
+          const int W = (nvec + nseg - 1) / nseg;
+          for (int p0 = 0; p0 < d.nz; p0 += P->seg3)
+            for (int g = 0; g < nseg; ++g)
+              for (int y0 = 0; y0 < d.ny; y0 += BY3) {
+                TileDesc tq;
+                tq.slot = sidx;
+                tq.x0 = g * W * 4;
+                tq.y0 = y0;
+                tq.p0 = p0;
+                tq.p1 = std::min(d.nz, p0 + P->seg3);
+                tq.local = 2 * local++;
+                base.push_back(tq);
+              }
+        }
         d.tile_count2 = local;
       }
       T->tt_live = (int)base.size();
@@ -774,6 +820,34 @@ StepArgs base_args(const nls_pool *P, const TileSet &T, int group = 0) {
   return a;
 }
 
+// Tile table, tile count and grid of the Lanczos passes j >= 1 of family L:
+// 2-D passes run one warp per (strip, sequence) of `lt` (or one TMA block per
+// tile of `tt`), 3-D FP32 passes one block per tile of `tt`, the other 3-D
+// passes one block per tile of `tiles` with both sequences.
+LaunchFn pass_args(const nls_pool *P, const TileSet &T, const Launch &L, StepArgs &b, int &grid) {
+  const int hc = P->step_hc;
+  grid = T.cap;
+  LaunchFn lf = L.lanczos[hc];
+  if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
+    b.tiles = T.d_tt;
+    b.ntiles = b.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
+    b.lt_stride = T.d_ntt1;
+    grid = T.tcap;
+    lf = P->ks.lanczos_tma;
+  } else if (P->dim == 2) {
+    b.tiles = T.d_lt;
+    b.ntiles = b.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
+    b.lt_stride = T.d_nlt1;
+    grid = T.lcap;
+  } else if (L.lanczos_tt[hc]) {
+    b.tiles = T.d_tt;
+    b.ntiles = b.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
+    b.lt_stride = T.d_ntt1;
+    grid = T.tcap;
+  }
+  return lf;
+}
+
 // One Krylov application family (first pass, Lanczos passes, f(T), final).
 int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &nk, cudaStream_t st) {
   const int grid = T.cap, hc = P->step_hc;
@@ -787,21 +861,9 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
     CK(L.first[hc](a, grid, st));
   }
   ++nk;
-  StepArgs b = a;  // 2-D passes: one warp per (strip, sequence) or one TMA block per tile
+  StepArgs b = a;
   int lgrid = grid;
-  LaunchFn lf = L.lanczos[hc];
-  if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
-    b.tiles = T.d_tt;
-    b.ntiles = a.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
-    b.lt_stride = T.d_ntt1;
-    lgrid = T.tcap;
-    lf = P->ks.lanczos_tma;
-  } else if (P->dim == 2) {
-    b.tiles = T.d_lt;
-    b.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
-    b.lt_stride = T.d_nlt1;
-    lgrid = T.lcap;
-  }
+  const LaunchFn lf = pass_args(P, T, L, b, lgrid);
   for (int j = 1; j <= P->k - 2; ++j) {
     b.j = j;
     LaunchFn fj = lf;
@@ -1523,7 +1585,6 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
   }
   if (P->main.nlist == 0) return fail(NLS_ERR_STATE, "no active slot");
   const Launch &L = P->cplx ? (P->method == NLS_NLSE_SS2 ? P->ks.ss2 : P->ks.sewi_a) : P->ks.kg;
-  const int hc = P->step_hc;
   // pass j over every main-step group, launched as the step launches it (the
   // two groups side by side on the pool stream and stream2)
   StepArgs args[2];
@@ -1537,19 +1598,7 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
     a.op_sign = P->cplx ? 1.0 : -1.0;
     a.nseq = P->method == NLS_NLSE_SS2 ? 1 : 2;
     int grid = T.cap;
-    LaunchFn lf = L.lanczos[hc];
-    if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
-      a.tiles = T.d_tt;
-      a.ntiles = a.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
-      a.lt_stride = T.d_ntt1;
-      grid = T.tcap;
-      lf = P->ks.lanczos_tma;
-    } else if (P->dim == 2) {
-      a.tiles = T.d_lt;
-      a.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
-      a.lt_stride = T.d_nlt1;
-      grid = T.lcap;
-    }
+    const LaunchFn lf = pass_args(P, T, L, a, grid);
     args[g] = a;
     grids[g] = grid;
     fns[g] = lf;

@@ -297,6 +297,10 @@ __global__ void __launch_bounds__(Geo<DIM>::NT) k_first(StepArgs a) {
           ringX[(sq * RX + ring(q, RX)) * G::PE + c.pidx(lx, ly)] = x;
           if (in && q >= c.p0 && q < c.p1 && lx >= 0 && lx < c.tx && ly >= 0 && ly < c.ty)
             ((E *)a.V)[(long long)(sq * a.kv) * a.vstride + e] = x;
+          // the row padding of V_0 is zero (the 3-D vector passes read whole 16-byte vectors)
+          else if (DIM == 3 && gx >= c.nx && gx < c.pitch && gy >= 0 && gy < c.ny && q >= c.p0 && q < c.p1 &&
+                   lx >= 0 && lx < c.tx && ly < c.ty)
+            ((E *)a.V)[(long long)(sq * a.kv) * a.vstride + c.gaddr(q, gx, gy)] = zero<E>();
         }
       }
     }
@@ -963,5 +967,6 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
 
 #include "nls_kernels_tail.cuh"
 #include "nls_warp2d.cuh"
+#include "nls_warp3d.cuh"
 
 }  // namespace nlsb

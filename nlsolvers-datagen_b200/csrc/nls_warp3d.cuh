@@ -1,0 +1,300 @@
+// 3-D fast path for real FP32 fields with c == 1: the Lanczos passes
+// j = 1 .. k-2 of the Gautschi step (kg_single.cuh:94-126 through
+// matfunc_real.hpp:190-313 and lanczos.hpp:208-267). Included inside
+// namespace nlsb, after the 2-D warp kernels whose vector helpers it uses.
+//
+// One block per (x strip, y band, z segment, sequence). Warp w of the block
+// owns grid row y = y0 - 2 + w of the strip for the whole segment and marches
+// its planes. Lanes hold 16-byte vectors as in the 2-D strips: lane 0 and
+// lane W+1 are halo lanes, and x-neighbours come through shuffles. Each warp
+// streams its own rows of V_{j-1} and V_{j-2} with 16-byte cp.async copies
+// into its ring in shared memory, PD3 planes ahead of the planes in use. The
+// y-neighbours of a row are read from the rings of the warps above and below,
+// and the neighbouring rows of v_j from a two-plane buffer. One block barrier
+// per plane orders the rings and the buffer.
+//
+// Roles by row: warps 0 and W3-1 (rows y0-2 and y0+BY3+1) only stream V_{j-1};
+// warps 1 and W3-2 (rows y0-1 and y0+BY3) also form v_j; the BY3 middle warps
+// form v_j, store V_j, and compute z = A v_j and the dots of their row.
+//
+// Plane q of the march forms v_j(q) = (sA L V_{j-1} - a sA V_{j-1} - d sB V_{j-2})(q) / b
+// for q = p0-1 .. p1 and z at plane q-1, as the 2-D rows do.
+constexpr int W3 = 16;         // warps per block
+constexpr int BY3 = W3 - 4;    // output rows per block
+constexpr int PD3 = 4;         // planes in flight beyond the three in use
+constexpr int RS3 = PD3 + 3;   // ring slots per warp and vector
+constexpr int RB3 = RS3 * 512; // ring bytes per warp and vector
+
+// Shared-memory accesses that other warps of the block observe after a
+// barrier (the memory clobber keeps them on their side of it).
+__device__ __forceinline__ void st_sh16(uint32_t saddr, const F4 &v) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(saddr), "f"(v.a.x), "f"(v.a.y), "f"(v.b.x),
+               "f"(v.b.y)
+               : "memory");
+}
+__device__ __forceinline__ F4 ld_sh16(uint32_t saddr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(saddr)
+               : "memory");
+  return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+
+struct Smem3 {
+  unsigned char A[W3][RS3][512];  // V_{j-1} rows, one ring per warp
+  unsigned char B[W3][RS3][512];  // V_{j-2} rows
+  unsigned char V[2][W3][512];    // v_j rows of the last two planes
+  double red[W3][6];              // per-warp dot sums
+  int last;
+};
+
+// Seven-point count-form operator on one row (c == 1): the five-point row
+// operator of lap4 plus the differences to the rows above and below (u, d).
+__device__ __forceinline__ F4 lap6(const F4 &m, const F4 &o, const F4 &p, const F4 &u, const F4 &d, float lft,
+                                   float rgt, const F4 &miss) {
+  const float2 nc0 = neg2(o.a), nc1 = neg2(o.b);
+  const float bm = __fsub_rn(o.a.x, lft), b0 = __fsub_rn(o.a.y, o.a.x), b1 = __fsub_rn(o.b.x, o.a.y),
+              b2 = __fsub_rn(o.b.y, o.b.x), b3 = __fsub_rn(rgt, o.b.y);
+  float2 s0 = make_float2(__fsub_rn(b0, bm), __fsub_rn(b1, b0));
+  float2 s1 = make_float2(__fsub_rn(b2, b1), __fsub_rn(b3, b2));
+  s0 = add2(s0, add2(add2(m.a, nc0), add2(p.a, nc0)));
+  s1 = add2(s1, add2(add2(m.b, nc1), add2(p.b, nc1)));
+  s0 = add2(s0, add2(add2(u.a, nc0), add2(d.a, nc0)));
+  s1 = add2(s1, add2(add2(u.b, nc1), add2(d.b, nc1)));
+  return F4{fma2(miss.a, o.a, s0), fma2(miss.b, o.b, s1)};
+}
+
+// Geometry of a 3-D strip: the balanced split of the row's 16-byte vectors
+// into strips of at most 30 output lanes (the same split as the 2-D strips).
+struct Strip3 {
+  int col0;      // first column of this lane's vector
+  bool ld;       // lane holds any in-grid column
+  bool io;       // lane owns output columns
+};
+__device__ __forceinline__ Strip3 make_strip3(int nx, int x0, int lane) {
+  const int nvec = (nx + 3) >> 2;
+  const int nseg = (nvec + 29) / 30;
+  const int wst = (nvec + nseg - 1) / nseg;
+  const int wcnt = min(wst, nvec - (x0 >> 2));
+  Strip3 S;
+  S.col0 = x0 + 4 * (lane - 1);
+  S.ld = lane < wcnt + 2 && S.col0 + 4 > 0 && S.col0 < nx;
+  S.io = lane >= 1 && lane <= wcnt && S.col0 < nx;
+  return S;
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const float *rowA, const float *rowB,
+                                             const float *safe, float *rowJ, long long PS, int p0, int p1, int nz,
+                                             bool ldA, bool ldB, bool form, bool outw, bool io, float2 CA,
+                                             float2 CB, const F4 &CSx, const F4 &OPx, const F4 &miss0,
+                                             double *acc) {
+  const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&sm.A[w][0][lane * 16]);
+  const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&sm.B[w][0][lane * 16]);
+  const uint32_t cellV = (uint32_t)__cvta_generic_to_shared(&sm.V[0][w][lane * 16]);
+  constexpr uint32_t VPL = W3 * 512;  // bytes of one plane of the v_j buffer
+  // fetch f: A plane p0-2+f, B plane p0-2+f (f >= 1); planes outside the grid
+  // are zero-filled; planes past the last one a kept result reads (A: p1+1,
+  // B: p1) are not fetched (warp-uniform test), so their slots keep stale rows
+  // that only discarded iterations read
+  const float *gA = rowA + (long long)(p0 - 2) * PS, *gB = rowB + (long long)(p0 - 2) * PS;
+  uint32_t soff = 0;
+  auto fetch = [&](int f) {
+    const int pl = p0 - 2 + f;
+    const bool inz = EDGE ? (pl >= 0 && pl < nz) : true;
+    if (pl <= p1 + 1) {
+      const bool ok = ldA && inz;
+      cp16z(cellA + soff, ok ? (const void *)gA : (const void *)safe, ok);
+    }
+    if (f >= 1 && pl <= p1 && form) {
+      const bool ok = ldB && inz;
+      cp16z(cellB + soff, ok ? (const void *)gB : (const void *)safe, ok);
+    }
+    gA += PS;
+    gB += PS;
+    soff += 512;
+    if (soff == (uint32_t)RB3) soff = 0;
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int f = 0; f < PD3 + 2; ++f) fetch(f);
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  cp_async_wait<PD3>();  // fetches 0, 1 landed (own rows; no other warp reads them yet)
+  F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2 = zero4;
+  F4 V0 = zero4, V1 = zero4, V2 = zero4;
+  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
+  // slot offsets of fetch it+1 (plane q) and it+2 (plane q+1)
+  uint32_t s1 = 512, s2 = 1024;
+  float *sp = rowJ + (long long)(p0 - 1) * PS;  // row of plane q in V_j
+  const int last_it = p1 - p0;                   // iterations 1 .. last_it store V_j, 2 .. last_it+1 reduce
+  const int nit = ((p1 - p0 + 2) + 2) / 3 * 3;
+#define NLSB_PLANE3(Am, Ac, Ap, Vm, Vc, Vn)                                                     \
+  {                                                                                           \
+    const int q = p0 - 1 + it;                                                                \
+    cp_async_wait<PD3 - 1>();                                                                 \
+    __syncthreads();                                                                          \
+    fetch(it + PD3 + 2);                                                                      \
+    Ap = lds16(cellA + s2);                                                                   \
+    if (form) {                                                                               \
+      const F4 up = ld_sh16(cellA - RB3 + s1), dn = ld_sh16(cellA + RB3 + s1);                    \
+      const F4 Bq = lds16(cellB + s1);                                                        \
+      const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
+      F4 miss = miss0;                                                                        \
+      if (EDGE) {                                                                             \
+        const float2 zm = f2(float((q == 0) + (q == nz - 1)));                                \
+        miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};                                      \
+      }                                                                                       \
+      const F4 wv = lap6(Am, Ac, Ap, up, dn, lft, rgt, miss);                                 \
+      Vn.a = fma2(CB, Bq.a, fma2(CA, Ac.a, mul2(CSx.a, wv.a)));                               \
+      Vn.b = fma2(CB, Bq.b, fma2(CA, Ac.b, mul2(CSx.b, wv.b)));                               \
+      if (EDGE) {                                                                             \
+        const float2 pv = f2((q >= 0 && q < nz) ? 1.f : 0.f);                                 \
+        Vn.a = mul2(Vn.a, pv);                                                                \
+        Vn.b = mul2(Vn.b, pv);                                                                \
+      }                                                                                       \
+      st_sh16(cellV + (it & 1) * VPL, Vn);                                                \
+      if (outw && io && it >= 1 && it <= last_it) f4_store(sp, Vn);                           \
+    }                                                                                         \
+    sp += PS;                                                                                 \
+    if (outw) {                                                                               \
+      const int r = q - 1;                                                                    \
+      const float lft = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                               \
+      const float rgt = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                             \
+      if (it >= 2 && it <= last_it + 1) {                                                     \
+        const uint32_t vprev = cellV + ((it - 1) & 1) * VPL;                                  \
+        const F4 vu = ld_sh16(vprev - 512), vd = ld_sh16(vprev + 512);                            \
+        F4 miss = miss0;                                                                      \
+        if (EDGE) {                                                                           \
+          const float2 zm = f2(float((r == 0) + (r == nz - 1)));                              \
+          miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};                                    \
+        }                                                                                     \
+        F4 z = lap6(Vm, Vc, Vn, vu, vd, lft, rgt, miss);                                      \
+        z.a = mul2(z.a, OPx.a);                                                               \
+        z.b = mul2(z.b, OPx.b);                                                               \
+        q0 = fma2(z.a, Am.a, fma2(z.b, Am.b, q0));                                            \
+        q1 = fma2(z.a, Vc.a, fma2(z.b, Vc.b, q1));                                            \
+        q2 = fma2(Am.a, Vc.a, fma2(Am.b, Vc.b, q2));                                          \
+        q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                              \
+        q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
+      }                                                                                       \
+    }                                                                                         \
+    s1 = s2;                                                                                  \
+    s2 = s2 + 512 == (uint32_t)RB3 ? 0u : s2 + 512;                                           \
+  }
+  for (int it0 = 0; it0 < nit; it0 += 3) {
+    int it = it0;
+    NLSB_PLANE3(A0, A1, A2, V1, V2, V0) ++it;
+    NLSB_PLANE3(A1, A2, A0, V2, V0, V1) ++it;
+    NLSB_PLANE3(A2, A0, A1, V0, V1, V2)
+    acc[0] += (double)(q0.x + q0.y);
+    acc[1] += (double)(q1.x + q1.y);
+    acc[2] += (double)(q2.x + q2.y);
+    acc[3] += (double)(q3.x + q3.y);
+    acc[4] += (double)(q4.x + q4.y);
+    q0 = q1 = q2 = q3 = q4 = f2(0.f);
+  }
+#undef NLSB_PLANE3
+  cp_async_wait<0>();
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem3_raw[];
+  Smem3 &sm = *reinterpret_cast<Smem3 *>(smem3_raw);
+  if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
+  const TileDesc t = a.tiles[blockIdx.x];
+  const SlotDesc &s = a.slots[t.slot];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = a.j, sq = t.local & 1;
+  const float opsc = float(a.op_sign * s.inv_h2);
+  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+  const double b0 = a.beta0[t.slot * 2 + sq];
+  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  const long long P = s.pitch, PS = P * ny;
+  const Strip3 S = make_strip3(nx, t.x0, lane);
+  const int y = t.y0 - 2 + w;
+  const bool yin = y >= 0 && y < ny;
+  const bool form = w >= 1 && w <= W3 - 2;
+  const bool outw = w >= 2 && w <= W3 - 3 && yin;
+  const bool hasB = j >= 2;
+  // rows outside the grid: zero coefficients make v_j zero there
+  const float yv = yin ? 1.f : 0.f;
+  const float cs = float(sA * L.inv_b) * opsc * yv;
+  const float2 CA = f2(float(-L.ar * sA * L.inv_b) * yv), CB = f2(hasB ? float(-L.dr * sB * L.inv_b) * yv : 0.f);
+  F4 CSx, OPx, miss0;
+  {
+    float v[4], m[4];
+    const float ym = float((y == 0) + (y == ny - 1));
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == nx - 1)) + ym;
+    }
+    CSx = F4{make_float2(v[0] * cs, v[1] * cs), make_float2(v[2] * cs, v[3] * cs)};
+    OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
+    miss0 = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  const long long vo = (long long)sq * a.kv;
+  const float *base = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
+  const long long row_off = s.off + (yin ? (long long)y * P : 0) + S.col0;
+  const float *rowA = (const float *)a.V + (vo + j - 1) * a.vstride + row_off;
+  const float *rowB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + row_off;
+  float *rowJ = (float *)a.V + (vo + j) * a.vstride + row_off;
+  const bool ldA = S.ld && yin, ldB = S.ld && yin && hasB;
+  double acc[5] = {0, 0, 0, 0, 0};
+  const int p0 = t.p0, p1 = t.p1;
+  if (p0 >= 2 && p1 <= nz - 2)
+    lz3f32_march<false>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
+                        CSx, OPx, miss0, acc);
+  else
+    lz3f32_march<true>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
+                       CSx, OPx, miss0, acc);
+  // the stored V_{j-1} is s0 v_{j-1} at j = 1 (V_0 holds the raw start vector)
+  acc[0] *= sA;
+  acc[2] *= sA;
+  const bool keep = outw && S.io;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double v = keep ? acc[q] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sm.red[w][q] = v;
+  }
+  __syncthreads();
+  constexpr int ND = 6;
+  const int TT = *a.lt_stride;
+  int *ticket = a.ticket + t.slot * 2 + sq;
+  double *part = a.part + (long long)j * a.part_stride;
+  if (threadIdx.x == 0) {
+    double tot[5] = {0, 0, 0, 0, 0};
+    for (int ww = 0; ww < W3; ++ww)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) tot[q] += sm.red[ww][q];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) __stcg(part + (long long)blockIdx.x * ND + q, tot[q]);
+    __stcg(part + (long long)blockIdx.x * ND + 5, 0.0);
+    // release: the partials are visible before the ticket; acquire: the last
+    // arrival observes every earlier block's partials
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;\n" : "=r"(old) : "l"(ticket) : "memory");
+    sm.last = old == s.tile_count2 - 1;
+  }
+  __syncthreads();
+  if (sm.last && w == 0) {
+    __threadfence();
+    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin2, s.tile_count2, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    tv[5] = L.n2;  // |v_{j-1}|^2, summed by the previous pass
+    if (lane == 0) {
+      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
+      *ticket = 0;
+    }
+  }
+}
