@@ -91,6 +91,8 @@ struct Launch {
   bool first_lt[2] = {false, false};  // the first pass runs on the pass tile table
   LaunchFn lanczos_lo[2] = {nullptr, nullptr};  // pass j = 1 with the low word of u (cosine sequence)
   bool lanczos_tt[2] = {false, false};  // 3-D passes run on the block table `tt`
+  bool first_tt[2] = {false, false};    // 3-D first pass on `tt` (one block per tile and sequence)
+  bool final_tt[2] = {false, false};    // 3-D final pass on the first section of `tt`
 };
 
 template <typename E, int SRC, bool HC>
@@ -206,6 +208,14 @@ bool use_k3() {
   }();
   return v != 0;
 }
+cudaError_t launch3_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
+  k3_first_f32<<<tiles, 32 * BY3, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch3_final_f32(const StepArgs &a, int tiles, cudaStream_t st) {
+  k3_final_f32<<<tiles, 32 * BY3, 0, st>>>(a);
+  return cudaGetLastError();
+}
 cudaError_t launch3_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   k3_lanczos_f32<1><<<tiles, 32 * W3, sizeof(Smem3), st>>>(a);
   return cudaGetLastError();
@@ -302,13 +312,17 @@ template <typename R> KSet make_real3() {
   KSet k;
   k.kg.first[0] = k.kg.first[1] = launch_first<3, R, 2, SRC_KG>;
   k.kg.lanczos[0] = k.kg.lanczos[1] = launch_lanczos<3, R, 2>;
+  k.kg.final_[0] = k.kg.final_[1] = launch_final<3, R, 2, FIN_KG>;
   if constexpr (sizeof(R) == 4) {
     if (use_k3()) {
+      k.kg.first[0] = launch3_first_f32;
+      k.kg.first_tt[0] = true;
       k.kg.lanczos[0] = launch3_lanczos_f32;
       k.kg.lanczos_tt[0] = true;
+      k.kg.final_[0] = launch3_final_f32;
+      k.kg.final_tt[0] = true;
     }
   }
-  k.kg.final_[0] = k.kg.final_[1] = launch_final<3, R, 2, FIN_KG>;
   k.sv[0] = k.sv[1] = launch_sv<3, R>;
   k.ftri = launch_ftri<R>;
   k.ring = launch_ring<R, 0>;
@@ -857,6 +871,12 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
     f.ntiles = a.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
     f.lt_stride = T.d_nlt1;
     CK(L.first[hc](f, T.lcap, st));
+  } else if (L.first_tt[hc]) {
+    StepArgs f = a;
+    f.tiles = T.d_tt;
+    f.ntiles = a.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
+    f.lt_stride = T.d_ntt1;
+    CK(L.first[hc](f, T.tcap, st));
   } else {
     CK(L.first[hc](a, grid, st));
   }
@@ -873,7 +893,15 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
   }
   CK(P->ks.ftri(a, P->max_slots, st));
   ++nk;
-  CK(L.final_[hc](a, grid, st));
+  if (L.final_tt[hc]) {
+    StepArgs f = a;
+    f.tiles = T.d_tt;
+    f.ntiles = T.d_ntt1;
+    f.lt_stride = T.d_ntt1;
+    CK(L.final_[hc](f, T.tcap, st));
+  } else {
+    CK(L.final_[hc](a, grid, st));
+  }
   ++nk;
   return NLS_OK;
 }

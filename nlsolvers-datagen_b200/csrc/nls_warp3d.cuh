@@ -298,3 +298,314 @@ __global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
     }
   }
 }
+
+// ------------------------------------------------ 3-D first and final passes
+// One warp per row of a block-table tile (warp w -> row y0 + w), marching the
+// segment's planes with the 16-byte lane vectors of the strip. Neither pass
+// forms a vector from another one's stencil, so the y-neighbours of a row are
+// simply loaded (L2 hits: the warps of those rows load them as their own) and
+// the z-neighbours come from a register window; the warps of a block never
+// wait for one another.
+__device__ __forceinline__ F4 ldrow(const float *p, bool ok) {
+  return ok ? f4_load(p) : F4{f2(0.f), f2(0.f)};
+}
+__device__ __forceinline__ F4 f4_mul(const F4 &x, const F4 &y) { return F4{mul2(x.a, y.a), mul2(x.b, y.b)}; }
+
+// Start vector of sequence SQ at one row: u (cosine sequence) or
+// g(u) = (p1 m + q1) u + (p3 m + q3) u^3 + (rm m + r0) xi (kg_single.cuh:103-111,
+// stochastic_phi4.cuh:19-77 with Philox keyed by (seed, step, point)).
+template <int SQ>
+__device__ __forceinline__ F4 src3(const F4 &u, const F4 &m, const SlotDesc &s, int step, int col0, int nx,
+                                   long long row_pt, bool noisy, bool ok) {
+  if (SQ == 0) return u;
+  F4 x = f4_g(u, m, f2(float(s.p1)), f2(float(s.q1)), f2(float(s.p3)), f2(float(s.q3)));
+  if (noisy && ok) {
+    float xs[4] = {x.a.x, x.a.y, x.b.x, x.b.y};
+    const float ms[4] = {m.a.x, m.a.y, m.b.x, m.b.y};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int xx = col0 + e;
+      if (xx >= 0 && xx < nx)
+        xs[e] += (float(s.rm) * ms[e] + float(s.r0)) *
+                 philox_normal<float>(s.seed, (uint32_t)step, (uint32_t)(row_pt + xx));
+    }
+    x = F4{make_float2(xs[0], xs[1]), make_float2(xs[2], xs[3])};
+  }
+  return x;
+}
+
+template <int SQ>
+__device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &s, const Strip3 &S, int y, int p0,
+                                             int p1, int step, const F4 &OPx, const F4 &miss0, double *acc) {
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  const long long P = s.pitch, PS = P * ny;
+  const long long row_off = s.off + (long long)y * P + S.col0;
+  const float *pU = (const float *)a.f.u_hi + row_off;
+  const float *pM = (const float *)a.f.m + row_off;
+  float *pV = (float *)a.V + (long long)(SQ * a.kv) * a.vstride + row_off;
+  const bool hu = y > 0, hd = y < ny - 1;
+  const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
+  auto xrow = [&](int q, long long dy) -> F4 {  // x at (y + dy, q)
+    const bool ok = S.ld && q >= 0 && q < nz;
+    const long long o = (long long)q * PS + dy * P;
+    const F4 u = ldrow(pU + o, ok);
+    const F4 m = SQ == 1 ? ldrow(pM + o, ok) : F4{f2(0.f), f2(0.f)};
+    return src3<SQ>(u, m, s, step, S.col0, nx, ((long long)q * ny + y + dy) * nx, noisy, ok);
+  };
+  F4 Xm = xrow(p0 - 1, 0), Xo = xrow(p0, 0);
+  float2 q1 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
+  for (int q = p0; q < p1; ++q) {
+    const F4 Xp = xrow(q + 1, 0);
+    const F4 Xu = hu ? xrow(q, -1) : F4{f2(0.f), f2(0.f)};
+    const F4 Xd = hd ? xrow(q, 1) : F4{f2(0.f), f2(0.f)};
+    const float lft = __shfl_up_sync(0xffffffffu, Xo.b.y, 1);
+    const float rgt = __shfl_down_sync(0xffffffffu, Xo.a.x, 1);
+    const float2 zm = f2(float((q == 0) + (q == nz - 1)));
+    const F4 miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};
+    const F4 z = f4_mul(lap6(Xm, Xo, Xp, Xu, Xd, lft, rgt, miss), OPx);
+    if (S.io) f4_store(pV + (long long)q * PS, Xo);
+    q1 = fma2(z.a, Xo.a, fma2(z.b, Xo.b, q1));
+    q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));
+    q4 = fma2(Xo.a, Xo.a, fma2(Xo.b, Xo.b, q4));
+    if (((q - p0) & 3) == 3) {
+      acc[1] += (double)(q1.x + q1.y);
+      acc[3] += (double)(q3.x + q3.y);
+      acc[4] += (double)(q4.x + q4.y);
+      q1 = q3 = q4 = f2(0.f);
+    }
+    Xm = Xo;
+    Xo = Xp;
+  }
+  acc[1] += (double)(q1.x + q1.y);
+  acc[3] += (double)(q3.x + q3.y);
+  acc[4] += (double)(q4.x + q4.y);
+}
+
+// Block partials of a pass (six values per warp in red[w], summed in warp
+// order) are stored at the block's entry of the pass region; the block that
+// takes the slot-sequence's last ticket sums the slot's entries in tile order
+// and publishes the scalars of pass j (lz_first and beta0 at j = 0).
+template <int NWB>
+__device__ __forceinline__ void block_publish3(const StepArgs &a, const SlotDesc &s, int slot, int sq, int j,
+                                               double (*red)[6], int *last_s, double n2_prev) {
+  constexpr int ND = 6;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *part = a.part + (long long)j * a.part_stride;
+  int *ticket = a.ticket + slot * 2 + sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot[ND] = {0, 0, 0, 0, 0, 0};
+    for (int ww = 0; ww < NWB; ++ww)
+#pragma unroll
+      for (int q = 0; q < ND; ++q) tot[q] += red[ww][q];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) __stcg(part + (long long)blockIdx.x * ND + q, tot[q]);
+    // release: the partials are visible before the ticket; acquire: the last
+    // arrival observes every earlier block's partials
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;\n" : "=r"(old) : "l"(ticket) : "memory");
+    *last_s = old == s.tile_count2 - 1;
+  }
+  __syncthreads();
+  if (*last_s && w == 0) {
+    __threadfence();
+    const int TT = *a.lt_stride;
+    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin2, s.tile_count2, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      if (j == 0) {
+        double b0;
+        a.scal[(slot * 2 + sq) * KMAX + 0] = lz_first<false>(tv, Eps<float>::v, b0);
+        a.beta0[slot * 2 + sq] = b0;
+      } else {
+        tv[5] = n2_prev;
+        a.scal[(slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
+      }
+      *ticket = 0;
+    }
+  }
+}
+
+static __global__ void __launch_bounds__(32 * BY3) k3_first_f32(StepArgs a) {
+  __shared__ double red[BY3][6];
+  __shared__ int last_s;
+  if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
+  const TileDesc t = a.tiles[blockIdx.x];
+  const SlotDesc &s = a.slots[t.slot];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int sq = t.local & 1, step = a.state[t.slot].step;
+  const int nx = s.nx, ny = s.ny, y = t.y0 + w;
+  const Strip3 S = make_strip3(nx, t.x0, lane);
+  const float opsc = float(a.op_sign * s.inv_h2);
+  F4 OPx, miss0;
+  {
+    float v[4], m[4];
+    const float ym = float((y == 0) + (y == ny - 1));
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == nx - 1)) + ym;
+    }
+    OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
+    miss0 = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (y < ny) {  // warp-uniform
+    if (sq == 0) first3_march<0>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc);
+    else first3_march<1>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc);
+  }
+  const bool keep = y < ny && S.io;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double v = keep ? acc[q] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w][q] = v;
+  }
+  block_publish3<BY3>(a, s, t.slot, sq, 0, red, &last_s, 0.0);
+}
+
+// y_seq = sum_{q < kv-1} W_q V_q + W_{kv-1} V_{kv-1} + Lam (A V_{kv-1}) for both
+// sequences, then the Gautschi update of kg_single.cuh:101-126 in increment
+// form: d+ = d + 2 y_cos + tau^2 y_sinc, u+ = u + d+, v = d+ / tau. Every load
+// of a plane (the window row of V_{kv-1} one plane ahead, its rows above and
+// below, the first eight V_q of each sequence and the fields) is issued before
+// the plane's arithmetic.
+static __global__ void __launch_bounds__(32 * BY3, 1) k3_final_f32(StepArgs a) {
+  constexpr int NB = 8;
+  __shared__ float Wsh[2][KMAX];
+  __shared__ float Lsh[2];
+  if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
+  const TileDesc t = a.tiles[blockIdx.x];
+  const SlotDesc &s = a.slots[t.slot];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int kv = a.kv;
+  if (threadIdx.x < 64) {
+    const int sq = threadIdx.x >> 5;
+    const FinalCoef &F = a.coef[t.slot * 2 + sq];
+    Wsh[sq][lane] = lane < kv ? F.wr32[lane] : 0.f;
+    if (lane == 0) Lsh[sq] = F.lam32[0];
+  }
+  __syncthreads();
+  const int nx = s.nx, ny = s.ny, nz = s.nz, y = t.y0 + w;
+  if (y >= ny) return;  // warp-uniform; no barrier follows
+  const int step = a.state[t.slot].step;
+  const Strip3 S = make_strip3(nx, t.x0, lane);
+  const float opsc = float(a.op_sign * s.inv_h2);
+  F4 xv, miss0;
+  {
+    float v[4], m[4];
+    const float ym = float((y == 0) + (y == ny - 1));
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == nx - 1)) + ym;
+    }
+    xv = F4{make_float2(v[0], v[1]), make_float2(v[2], v[3])};
+    miss0 = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
+  }
+  const long long P = s.pitch, PS = P * ny;
+  const long long row_off = s.off + (long long)y * P + S.col0;
+  const float *VL0 = (const float *)a.V + (long long)(kv - 1) * a.vstride + row_off;
+  const float *VL1 = (const float *)a.V + (long long)(a.kv + kv - 1) * a.vstride + row_off;
+  const float *Vb0 = (const float *)a.V + row_off;
+  const float *Vb1 = (const float *)a.V + (long long)a.kv * a.vstride + row_off;
+  float *pH = (float *)a.f.u_hi + row_off;
+  float *pL = (float *)a.f.u_lo + row_off;
+  float *pD = (float *)a.f.d + row_off;
+  const bool hu = y > 0, hd = y < ny - 1, ld = S.ld, io = S.io;
+  const float2 OP = f2(opsc), LA0 = f2(Lsh[0]), LA1 = f2(Lsh[1]);
+  const float2 WL0 = f2(Wsh[0][kv - 1]), WL1 = f2(Wsh[1][kv - 1]);
+  const float dt = float(s.dt), t2 = dt * dt;
+  int fr = 0;
+  const bool snap = snap_step(s, step, fr);
+  double *SN = a.f.snap + s.snap_off + (long long)fr * 2 * s.n;
+  const int p0 = t.p0, p1 = t.p1;
+  auto okp = [&](int q) { return ld && q >= 0 && q < nz; };
+  F4 Lm0, Lo0 = ldrow(VL0 + (long long)(p0 - 1) * PS, okp(p0 - 1)), Lp0 = ldrow(VL0 + (long long)p0 * PS, okp(p0));
+  F4 Lm1, Lo1 = ldrow(VL1 + (long long)(p0 - 1) * PS, okp(p0 - 1)), Lp1 = ldrow(VL1 + (long long)p0 * PS, okp(p0));
+  for (int q = p0; q < p1; ++q) {
+    const long long o = (long long)q * PS;
+    // ---- the plane's loads
+    const F4 Ln0 = ldrow(VL0 + o + PS, okp(q + 1)), Ln1 = ldrow(VL1 + o + PS, okp(q + 1));
+    const F4 U0 = ldrow(VL0 + o - P, ld && hu), D0 = ldrow(VL0 + o + P, ld && hd);
+    const F4 U1 = ldrow(VL1 + o - P, ld && hu), D1 = ldrow(VL1 + o + P, ld && hd);
+    F4 vb0[NB], vb1[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      vb0[i] = ldrow(Vb0 + o + (long long)i * a.vstride, io && i < kv - 1);
+      vb1[i] = ldrow(Vb1 + o + (long long)i * a.vstride, io && i < kv - 1);
+    }
+    const F4 fh = ldrow(pH + o, io), fl = ldrow(pL + o, io), fd = ldrow(pD + o, io);
+    // ---- arithmetic
+    Lm0 = Lo0; Lo0 = Lp0; Lp0 = Ln0;
+    Lm1 = Lo1; Lo1 = Lp1; Lp1 = Ln1;
+    const float2 zm = f2(float((q == 0) + (q == nz - 1)));
+    const F4 miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};
+    F4 y0, y1;
+    {
+      const float lft = __shfl_up_sync(0xffffffffu, Lo0.b.y, 1);
+      const float rgt = __shfl_down_sync(0xffffffffu, Lo0.a.x, 1);
+      const F4 z = lap6(Lm0, Lo0, Lp0, U0, D0, lft, rgt, miss);
+      y0 = F4{fma2(WL0, Lo0.a, mul2(LA0, mul2(OP, z.a))), fma2(WL0, Lo0.b, mul2(LA0, mul2(OP, z.b)))};
+    }
+    {
+      const float lft = __shfl_up_sync(0xffffffffu, Lo1.b.y, 1);
+      const float rgt = __shfl_down_sync(0xffffffffu, Lo1.a.x, 1);
+      const F4 z = lap6(Lm1, Lo1, Lp1, U1, D1, lft, rgt, miss);
+      y1 = F4{fma2(WL1, Lo1.a, mul2(LA1, mul2(OP, z.a))), fma2(WL1, Lo1.b, mul2(LA1, mul2(OP, z.b)))};
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      const float2 w0 = f2(Wsh[0][i]), w1 = f2(Wsh[1][i]);
+      y0 = F4{fma2(w0, vb0[i].a, y0.a), fma2(w0, vb0[i].b, y0.b)};
+      y1 = F4{fma2(w1, vb1[i].a, y1.a), fma2(w1, vb1[i].b, y1.b)};
+    }
+    if (kv - 1 > NB && io) {
+      for (int q0 = NB; q0 < kv - 1; q0 += NB) {
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+          vb0[i] = ldrow(Vb0 + o + (long long)(q0 + i) * a.vstride, q0 + i < kv - 1);
+          vb1[i] = ldrow(Vb1 + o + (long long)(q0 + i) * a.vstride, q0 + i < kv - 1);
+        }
+#pragma unroll
+        for (int i = 0; i < NB; ++i) {
+          const float2 w0 = f2(Wsh[0][q0 + i]), w1 = f2(Wsh[1][q0 + i]);
+          y0 = F4{fma2(w0, vb0[i].a, y0.a), fma2(w0, vb0[i].b, y0.b)};
+          y1 = F4{fma2(w1, vb1[i].a, y1.a), fma2(w1, vb1[i].b, y1.b)};
+        }
+      }
+    }
+    if (io) {
+      float h[4] = {fh.a.x, fh.a.y, fh.b.x, fh.b.y}, l[4] = {fl.a.x, fl.a.y, fl.b.x, fl.b.y};
+      const float d[4] = {fd.a.x, fd.a.y, fd.b.x, fd.b.y};
+      const float c0[4] = {y0.a.x, y0.a.y, y0.b.x, y0.b.y}, c1[4] = {y1.a.x, y1.a.y, y1.b.x, y1.b.y};
+      const float m[4] = {xv.a.x, xv.a.y, xv.b.x, xv.b.y};
+      float dn[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float dp = (d[e] + 2.f * (c0[e] * m[e])) + t2 * (c1[e] * m[e]);
+        comp_add(h[e], l[e], dp);
+        dn[e] = dp;
+      }
+      f4_store(pH + o, F4{make_float2(h[0], h[1]), make_float2(h[2], h[3])});
+      f4_store(pL + o, F4{make_float2(l[0], l[1]), make_float2(l[2], l[3])});
+      f4_store(pD + o, F4{make_float2(dn[0], dn[1]), make_float2(dn[2], dn[3])});
+      if (snap) {
+        const long long rp = ((long long)q * ny + y) * nx;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int x = S.col0 + e;
+          if (x < nx) {
+            SN[rp + x] = (double)h[e] + (double)l[e];
+            SN[s.n + rp + x] = (double)dn[e] / s.dt;
+          }
+        }
+      }
+    }
+  }
+}
