@@ -287,19 +287,28 @@ def run_small(args, lrank):
     32-row segments), warmup + steps only; the case the ncu captures profile
     (16: ~0.2 GB, 64: ~0.7 GB on the GPU, both above the 126 MB L2)."""
     import nlsb200 as nl
+    from nlsb200 import workloads as W
     from nlsb200.solver import FP32, KG_GAUTSCHI, Pool
     nl.lib().nls_set_device(lrank)
     B, k = args.batch, 10
-    cases = make_batch(B, 0, k)
-    cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
-    pool = Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg)
+    dim = 3 if args.dim3 else 2
+    if dim == 3:
+        # KG 3-D Gautschi boxes of dim3^3 on [-10,10]^3, dt = 0.01, 40 snapshots
+        cases = [W.kg_case(args.dim3, 10.0, T=100.0, nt=10000, ns=40, k=k, seed=i, dim=3, precision=FP32)
+                 for i in range(B)]
+        cap = sum(((s.nx + 31) // 32 * 32) * s.ny * s.nz for s, *_ in cases) + 256 * B
+    else:
+        cases = make_batch(B, 0, k)
+        cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
+    pool = Pool(KG_GAUTSCHI, dim, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg)
     for cs in cases:
         assert pool.admit(*cs) is not None
     pool.step(args.warmup)
     ms = pool.step_timed(args.steps)
     pool.sync()
     pass_ms, _ = pool.time_pass(2, 20)
-    print(json.dumps({"small": True, "batch": B, "k": k, "seg": args.seg, "ms_per_step": ms / args.steps,
+    print(json.dumps({"small": True, "dim": dim, "n": cases[0][0].nx, "batch": B, "k": k, "seg": args.seg,
+                      "ms_per_step": ms / args.steps,
                       "pass_ms": pass_ms, "kernels_per_step": pool.kernels_per_step()}), flush=True)
     pool.close()
     return 0
@@ -439,7 +448,9 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
-    ap.add_argument("--seg", type=int, default=32, help="segment rows of the --small case")
+    ap.add_argument("--seg", type=int, default=32, help="segment rows (planes in 3-D) of the --small case")
+    ap.add_argument("--dim3", type=int, default=0,
+                    help="--small case as KG 3-D boxes of DIM3^3 points (0: the 2-D 300^2 workload)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -8,7 +8,7 @@
 // its planes. Lanes hold 16-byte vectors as in the 2-D strips: lane 0 and
 // lane W+1 are halo lanes, and x-neighbours come through shuffles. Each warp
 // streams its own rows of V_{j-1} and V_{j-2} with 16-byte cp.async copies
-// into its ring in shared memory, PD3 planes ahead of the planes in use. The
+// into its ring in shared memory, PD planes ahead of the planes in use. The
 // y-neighbours of a row are read from the rings of the warps above and below,
 // and the neighbouring rows of v_j from a two-plane buffer. One block barrier
 // per plane orders the rings and the buffer.
@@ -21,9 +21,8 @@
 // for q = p0-1 .. p1 and z at plane q-1, as the 2-D rows do.
 constexpr int W3 = 16;         // warps per block
 constexpr int BY3 = W3 - 4;    // output rows per block
-constexpr int PD3 = 4;         // planes in flight beyond the three in use
-constexpr int RS3 = PD3 + 3;   // ring slots per warp and vector
-constexpr int RB3 = RS3 * 512; // ring bytes per warp and vector
+// PD (template): planes in flight beyond the three in use; ring slots per warp
+// and vector RS = PD + 3 of 512 bytes.
 
 // Shared-memory accesses that other warps of the block observe after a
 // barrier (the memory clobber keeps them on their side of it).
@@ -41,9 +40,10 @@ __device__ __forceinline__ F4 ld_sh16(uint32_t saddr) {
   return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
 }
 
-struct Smem3 {
-  unsigned char A[W3][RS3][512];  // V_{j-1} rows, one ring per warp
-  unsigned char B[W3][RS3][512];  // V_{j-2} rows
+template <int PD> struct Smem3 {
+  static constexpr int RS = PD + 3;
+  unsigned char A[W3][RS][512];   // V_{j-1} rows, one ring per warp
+  unsigned char B[W3][RS][512];   // V_{j-2} rows
   unsigned char V[2][W3][512];    // v_j rows of the last two planes
   double red[W3][6];              // per-warp dot sums
   int last;
@@ -84,8 +84,8 @@ __device__ __forceinline__ Strip3 make_strip3(int nx, int x0, int lane) {
   return S;
 }
 
-template <bool EDGE>
-__device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const float *rowA, const float *rowB,
+template <bool EDGE, int PD3>
+__device__ __forceinline__ void lz3f32_march(Smem3<PD3> &sm, int w, int lane, const float *rowA, const float *rowB,
                                              const float *safe, float *rowJ, long long PS, int p0, int p1, int nz,
                                              bool ldA, bool ldB, bool form, bool outw, bool io, float2 CA,
                                              float2 CB, const F4 &CSx, const F4 &OPx, const F4 &miss0,
@@ -94,6 +94,7 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
   const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&sm.B[w][0][lane * 16]);
   const uint32_t cellV = (uint32_t)__cvta_generic_to_shared(&sm.V[0][w][lane * 16]);
   constexpr uint32_t VPL = W3 * 512;  // bytes of one plane of the v_j buffer
+  constexpr int RB3 = Smem3<PD3>::RS * 512;  // ring bytes per warp and vector
   // fetch f: A plane p0-2+f, B plane p0-2+f (f >= 1); planes outside the grid
   // are zero-filled; planes past the last one a kept result reads (A: p1+1,
   // B: p1) are not fetched (warp-uniform test), so their slots keep stale rows
@@ -199,10 +200,10 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
   cp_async_wait<0>();
 }
 
-template <int MINB>
+template <int MINB, int PD3>
 __global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem3_raw[];
-  Smem3 &sm = *reinterpret_cast<Smem3 *>(smem3_raw);
+  Smem3<PD3> &sm = *reinterpret_cast<Smem3<PD3> *>(smem3_raw);
   if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
   const TileDesc t = a.tiles[blockIdx.x];
   const SlotDesc &s = a.slots[t.slot];
@@ -249,10 +250,10 @@ __global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
   double acc[5] = {0, 0, 0, 0, 0};
   const int p0 = t.p0, p1 = t.p1;
   if (p0 >= 2 && p1 <= nz - 2)
-    lz3f32_march<false>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
+    lz3f32_march<false, PD3>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
                         CSx, OPx, miss0, acc);
   else
-    lz3f32_march<true>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
+    lz3f32_march<true, PD3>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
                        CSx, OPx, miss0, acc);
   // the stored V_{j-1} is s0 v_{j-1} at j = 1 (V_0 holds the raw start vector)
   acc[0] *= sA;
