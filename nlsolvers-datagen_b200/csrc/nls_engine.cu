@@ -213,14 +213,11 @@ cudaError_t launch3_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   return cudaGetLastError();
 }
 cudaError_t launch3_final_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k3_final_f32<<<tiles, 32 * BY3, 0, st>>>(a);
+  k3_final_f32<<<2 * tiles, 32 * FH3, 0, st>>>(a);
   return cudaGetLastError();
 }
-// One block of 16 warps per SM (116 registers); four planes in flight. Measured
-// at 16 x 220^3: two planes 1.58, three 1.56, four and six 1.55 ms per pass;
-// two blocks per SM (64 registers, spilling) 2.09 ms.
 cudaError_t launch3_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k3_lanczos_f32<1, 4><<<tiles, 32 * W3, sizeof(Smem3<4>), st>>>(a);
+  k3_lanczos_f32<<<tiles, 32 * W3, sizeof(Smem3), st>>>(a);
   return cudaGetLastError();
 }
 
@@ -288,7 +285,7 @@ struct KSet {
 template <int DIM, typename R> cudaError_t attrs_real() {
   cudaError_t e;
   if constexpr (DIM == 3 && sizeof(R) == 4) {
-    if ((e = set_smem(k3_lanczos_f32<1, 4>, sizeof(Smem3<4>)))) return e;
+    if ((e = set_smem(k3_lanczos_f32, sizeof(Smem3)))) return e;
   }
   if ((e = set_smem(k_first<DIM, R, 2, SRC_KG>, smem_first<DIM, R, 2>()))) return e;
   if ((e = set_smem(k_lanczos<DIM, R, 2>, smem_lanczos<DIM, R, 2>()))) return e;
@@ -488,7 +485,8 @@ struct TileSet {
   int lcap = 0;
   int lt_count2 = 0;  // host copy of 2 * live (source of the async upload)
   std::vector<TileDesc> lt;
-  // 2-D TMA passes: tiles of <= 512 columns x segment rows, one section per sequence
+  // block tables, one section per sequence: 2-D TMA passes (tiles of <= 512
+  // columns x segment rows) or the 3-D FP32 passes (strip x band x segment)
   TileDesc *d_tt = nullptr;
   int *d_ntt1 = nullptr, *d_ntt2 = nullptr;
   int tcap = 0, tt_live = 0, tt_count2 = 0;
@@ -530,7 +528,10 @@ struct nls_pool {
   std::vector<SlotHost> hs;
   std::vector<SlotDesc> sd;
   bool tables_dirty = true;
-  int seg2 = 32, seg3 = 32;  // march lengths (rows in 2-D, planes in 3-D)
+  // 3-D: 88 planes (90 march iterations, a multiple of the 6-plane unroll);
+  // 16 x 220^3 measured 16.37 / 15.81 / 15.33 / 15.28 / 15.14 / 15.20 ms per
+  // step at 32 / 40 / 58 / 70 / 88 / 110 planes
+  int seg2 = 32, seg3 = 88;  // march lengths (rows in 2-D, planes in 3-D)
   cudaStream_t stream = nullptr, copy_stream = nullptr, stream2 = nullptr;
   cudaEvent_t ev_step = nullptr, ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = true;

@@ -8,9 +8,9 @@
 // its planes. Lanes hold 16-byte vectors as in the 2-D strips: lane 0 and
 // lane W+1 are halo lanes, and x-neighbours come through shuffles. Each warp
 // streams its own rows of V_{j-1} and V_{j-2} with 16-byte cp.async copies
-// into its ring in shared memory, PD planes ahead of the planes in use. The
+// into its ring in shared memory, PD3 planes ahead of the planes in use. The
 // y-neighbours of a row are read from the rings of the warps above and below,
-// and the neighbouring rows of v_j from a two-plane buffer. One block barrier
+// and the neighbouring rows of v_j from a three-plane buffer. One block barrier
 // per plane orders the rings and the buffer.
 //
 // Roles by row: warps 0 and W3-1 (rows y0-2 and y0+BY3+1) only stream V_{j-1};
@@ -19,10 +19,11 @@
 //
 // Plane q of the march forms v_j(q) = (sA L V_{j-1} - a sA V_{j-1} - d sB V_{j-2})(q) / b
 // for q = p0-1 .. p1 and z at plane q-1, as the 2-D rows do.
-constexpr int W3 = 16;         // warps per block
+constexpr int W3 = 24;         // warps per block
 constexpr int BY3 = W3 - 4;    // output rows per block
-// PD (template): planes in flight beyond the three in use; ring slots per warp
-// and vector RS = PD + 3 of 512 bytes.
+constexpr int PD3 = 3;         // planes in flight beyond the three in use
+constexpr int RS3 = PD3 + 3;   // ring slots per warp and vector (the unroll factor of the march)
+constexpr int NV3 = 3;         // planes of the v_j buffer
 
 // Shared-memory accesses that other warps of the block observe after a
 // barrier (the memory clobber keeps them on their side of it).
@@ -40,11 +41,10 @@ __device__ __forceinline__ F4 ld_sh16(uint32_t saddr) {
   return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
 }
 
-template <int PD> struct Smem3 {
-  static constexpr int RS = PD + 3;
-  unsigned char A[W3][RS][512];   // V_{j-1} rows, one ring per warp
-  unsigned char B[W3][RS][512];   // V_{j-2} rows
-  unsigned char V[2][W3][512];    // v_j rows of the last two planes
+struct Smem3 {
+  unsigned char A[W3][RS3][512];  // V_{j-1} rows, one ring per warp
+  unsigned char B[W3][RS3][512];  // V_{j-2} rows
+  unsigned char V[NV3][W3][512];  // v_j rows of the last three planes
   double red[W3][6];              // per-warp dot sums
   int last;
 };
@@ -84,62 +84,67 @@ __device__ __forceinline__ Strip3 make_strip3(int nx, int x0, int lane) {
   return S;
 }
 
-template <bool EDGE, int PD3>
-__device__ __forceinline__ void lz3f32_march(Smem3<PD3> &sm, int w, int lane, const float *rowA, const float *rowB,
+// The march keeps no plane of V_{j-1} or v_j in registers across planes: the
+// warp re-reads its own rows from its ring and from the v_j buffer, which keeps
+// the register count low enough for one block of 24 warps per SM. The loop is
+// unrolled by the ring length RS3 (a multiple of the buffer length NV3), so
+// every ring and buffer offset is a compile-time constant.
+template <bool EDGE>
+__device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const float *rowA, const float *rowB,
                                              const float *safe, float *rowJ, long long PS, int p0, int p1, int nz,
                                              bool ldA, bool ldB, bool form, bool outw, bool io, float2 CA,
                                              float2 CB, const F4 &CSx, const F4 &OPx, const F4 &miss0,
                                              double *acc) {
+  static_assert(RS3 % NV3 == 0, "unroll by the ring length must cycle the v_j buffer");
   const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&sm.A[w][0][lane * 16]);
   const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&sm.B[w][0][lane * 16]);
   const uint32_t cellV = (uint32_t)__cvta_generic_to_shared(&sm.V[0][w][lane * 16]);
-  constexpr uint32_t VPL = W3 * 512;  // bytes of one plane of the v_j buffer
-  constexpr int RB3 = Smem3<PD3>::RS * 512;  // ring bytes per warp and vector
-  // fetch f: A plane p0-2+f, B plane p0-2+f (f >= 1); planes outside the grid
-  // are zero-filled; planes past the last one a kept result reads (A: p1+1,
-  // B: p1) are not fetched (warp-uniform test), so their slots keep stale rows
-  // that only discarded iterations read
+  constexpr uint32_t VPL = W3 * 512;   // bytes of one plane of the v_j buffer
+  constexpr uint32_t RB = RS3 * 512;   // ring bytes per warp and vector
+  // fetch f: A plane p0-2+f, B plane p0-2+f (f >= 1) into slot f % RS3; planes
+  // outside the grid are zero-filled; planes past the last one a kept result
+  // reads (A: p1+1, B: p1) are not fetched (warp-uniform test), so their slots
+  // keep stale rows that only discarded iterations read
   const float *gA = rowA + (long long)(p0 - 2) * PS, *gB = rowB + (long long)(p0 - 2) * PS;
-  uint32_t soff = 0;
-  auto fetch = [&](int f) {
+  auto fetch = [&](int f, uint32_t slot) {
     const int pl = p0 - 2 + f;
     const bool inz = EDGE ? (pl >= 0 && pl < nz) : true;
     if (pl <= p1 + 1) {
       const bool ok = ldA && inz;
-      cp16z(cellA + soff, ok ? (const void *)gA : (const void *)safe, ok);
+      cp16z(cellA + slot, ok ? (const void *)gA : (const void *)safe, ok);
     }
     if (f >= 1 && pl <= p1 && form) {
       const bool ok = ldB && inz;
-      cp16z(cellB + soff, ok ? (const void *)gB : (const void *)safe, ok);
+      cp16z(cellB + slot, ok ? (const void *)gB : (const void *)safe, ok);
     }
     gA += PS;
     gB += PS;
-    soff += 512;
-    if (soff == (uint32_t)RB3) soff = 0;
     cp_async_commit();
   };
 #pragma unroll
-  for (int f = 0; f < PD3 + 2; ++f) fetch(f);
-  const F4 zero4 = F4{f2(0.f), f2(0.f)};
-  cp_async_wait<PD3>();  // fetches 0, 1 landed (own rows; no other warp reads them yet)
-  F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2 = zero4;
-  F4 V0 = zero4, V1 = zero4, V2 = zero4;
+  for (int f = 0; f < PD3 + 2; ++f) fetch(f, f * 512);
   float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
-  // slot offsets of fetch it+1 (plane q) and it+2 (plane q+1)
-  uint32_t s1 = 512, s2 = 1024;
   float *sp = rowJ + (long long)(p0 - 1) * PS;  // row of plane q in V_j
   const int last_it = p1 - p0;                   // iterations 1 .. last_it store V_j, 2 .. last_it+1 reduce
-  const int nit = ((p1 - p0 + 2) + 2) / 3 * 3;
-#define NLSB_PLANE3(Am, Ac, Ap, Vm, Vc, Vn)                                                     \
+  const int nit = (p1 - p0 + 2 + RS3 - 1) / RS3 * RS3;
+  // iteration it = it0 + K: A planes q-1, q, q+1 in slots K, K+1, K+2 (mod RS3),
+  // B plane q in slot K+1; v_j(q) into buffer plane K % NV3, v_j(q-1) and
+  // v_j(q-2) in planes (K+2) % NV3 and (K+1) % NV3
+#define NLSB_PLANE3(K)                                                                        \
   {                                                                                           \
+    const int it = it0 + (K);                                                                 \
     const int q = p0 - 1 + it;                                                                \
+    constexpr uint32_t sm1 = ((K) % RS3) * 512, s0 = (((K) + 1) % RS3) * 512,                 \
+                       sp1 = (((K) + 2) % RS3) * 512, sf = (((K) + PD3 + 2) % RS3) * 512;     \
+    constexpr uint32_t vn = ((K) % NV3) * VPL, vc = (((K) + 2) % NV3) * VPL,                  \
+                       vm = (((K) + 1) % NV3) * VPL;                                          \
     cp_async_wait<PD3 - 1>();                                                                 \
     __syncthreads();                                                                          \
-    fetch(it + PD3 + 2);                                                                      \
-    Ap = lds16(cellA + s2);                                                                   \
+    fetch(it + PD3 + 2, sf);                                                                  \
     if (form) {                                                                               \
-      const F4 up = ld_sh16(cellA - RB3 + s1), dn = ld_sh16(cellA + RB3 + s1);                    \
-      const F4 Bq = lds16(cellB + s1);                                                        \
+      const F4 Am = lds16(cellA + sm1), Ac = lds16(cellA + s0), Ap = lds16(cellA + sp1);      \
+      const F4 up = ld_sh16(cellA - RB + s0), dn = ld_sh16(cellA + RB + s0);                  \
+      const F4 Bq = lds16(cellB + s0);                                                        \
       const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
       const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
       F4 miss = miss0;                                                                        \
@@ -148,6 +153,7 @@ __device__ __forceinline__ void lz3f32_march(Smem3<PD3> &sm, int w, int lane, co
         miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};                                      \
       }                                                                                       \
       const F4 wv = lap6(Am, Ac, Ap, up, dn, lft, rgt, miss);                                 \
+      F4 Vn;                                                                                  \
       Vn.a = fma2(CB, Bq.a, fma2(CA, Ac.a, mul2(CSx.a, wv.a)));                               \
       Vn.b = fma2(CB, Bq.b, fma2(CA, Ac.b, mul2(CSx.b, wv.b)));                               \
       if (EDGE) {                                                                             \
@@ -155,23 +161,20 @@ __device__ __forceinline__ void lz3f32_march(Smem3<PD3> &sm, int w, int lane, co
         Vn.a = mul2(Vn.a, pv);                                                                \
         Vn.b = mul2(Vn.b, pv);                                                                \
       }                                                                                       \
-      st_sh16(cellV + (it & 1) * VPL, Vn);                                                \
+      st_sh16(cellV + vn, Vn);                                                                \
       if (outw && io && it >= 1 && it <= last_it) f4_store(sp, Vn);                           \
-    }                                                                                         \
-    sp += PS;                                                                                 \
-    if (outw) {                                                                               \
-      const int r = q - 1;                                                                    \
-      const float lft = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                               \
-      const float rgt = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                             \
-      if (it >= 2 && it <= last_it + 1) {                                                     \
-        const uint32_t vprev = cellV + ((it - 1) & 1) * VPL;                                  \
-        const F4 vu = ld_sh16(vprev - 512), vd = ld_sh16(vprev + 512);                            \
-        F4 miss = miss0;                                                                      \
+      if (outw && it >= 2 && it <= last_it + 1) {                                             \
+        const int r = q - 1;                                                                  \
+        const F4 Vm = lds16(cellV + vm), Vc = lds16(cellV + vc);                              \
+        const F4 vu = ld_sh16(cellV + vc - 512), vd = ld_sh16(cellV + vc + 512);              \
+        const float lv = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                              \
+        const float rv = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                            \
+        F4 mz = miss0;                                                                        \
         if (EDGE) {                                                                           \
           const float2 zm = f2(float((r == 0) + (r == nz - 1)));                              \
-          miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};                                    \
+          mz = F4{add2(miss0.a, zm), add2(miss0.b, zm)};                                      \
         }                                                                                     \
-        F4 z = lap6(Vm, Vc, Vn, vu, vd, lft, rgt, miss);                                      \
+        F4 z = lap6(Vm, Vc, Vn, vu, vd, lv, rv, mz);                                          \
         z.a = mul2(z.a, OPx.a);                                                               \
         z.b = mul2(z.b, OPx.b);                                                               \
         q0 = fma2(z.a, Am.a, fma2(z.b, Am.b, q0));                                            \
@@ -181,29 +184,27 @@ __device__ __forceinline__ void lz3f32_march(Smem3<PD3> &sm, int w, int lane, co
         q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
       }                                                                                       \
     }                                                                                         \
-    s1 = s2;                                                                                  \
-    s2 = s2 + 512 == (uint32_t)RB3 ? 0u : s2 + 512;                                           \
+    sp += PS;                                                                                 \
   }
-  for (int it0 = 0; it0 < nit; it0 += 3) {
-    int it = it0;
-    NLSB_PLANE3(A0, A1, A2, V1, V2, V0) ++it;
-    NLSB_PLANE3(A1, A2, A0, V2, V0, V1) ++it;
-    NLSB_PLANE3(A2, A0, A1, V0, V1, V2)
-    acc[0] += (double)(q0.x + q0.y);
-    acc[1] += (double)(q1.x + q1.y);
-    acc[2] += (double)(q2.x + q2.y);
-    acc[3] += (double)(q3.x + q3.y);
-    acc[4] += (double)(q4.x + q4.y);
-    q0 = q1 = q2 = q3 = q4 = f2(0.f);
+#define NLSB_FLUSH3                       \
+  acc[0] += (double)(q0.x + q0.y);        \
+  acc[1] += (double)(q1.x + q1.y);        \
+  acc[2] += (double)(q2.x + q2.y);        \
+  acc[3] += (double)(q3.x + q3.y);        \
+  acc[4] += (double)(q4.x + q4.y);        \
+  q0 = q1 = q2 = q3 = q4 = f2(0.f);
+  for (int it0 = 0; it0 < nit; it0 += RS3) {
+    NLSB_PLANE3(0) NLSB_PLANE3(1) NLSB_PLANE3(2) NLSB_FLUSH3
+    NLSB_PLANE3(3) NLSB_PLANE3(4) NLSB_PLANE3(5) NLSB_FLUSH3
   }
+#undef NLSB_FLUSH3
 #undef NLSB_PLANE3
   cp_async_wait<0>();
 }
 
-template <int MINB, int PD3>
-__global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
+static __global__ void __launch_bounds__(32 * W3, 1) k3_lanczos_f32(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem3_raw[];
-  Smem3<PD3> &sm = *reinterpret_cast<Smem3<PD3> *>(smem3_raw);
+  Smem3 &sm = *reinterpret_cast<Smem3 *>(smem3_raw);
   if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
   const TileDesc t = a.tiles[blockIdx.x];
   const SlotDesc &s = a.slots[t.slot];
@@ -250,10 +251,10 @@ __global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
   double acc[5] = {0, 0, 0, 0, 0};
   const int p0 = t.p0, p1 = t.p1;
   if (p0 >= 2 && p1 <= nz - 2)
-    lz3f32_march<false, PD3>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
+    lz3f32_march<false>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
                         CSx, OPx, miss0, acc);
   else
-    lz3f32_march<true, PD3>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
+    lz3f32_march<true>(sm, w, lane, rowA, rowB, base, rowJ, PS, p0, p1, nz, ldA, ldB, form, outw, S.io, CA, CB,
                        CSx, OPx, miss0, acc);
   // the stored V_{j-1} is s0 v_{j-1} at j = 1 (V_0 holds the raw start vector)
   acc[0] *= sA;
@@ -301,8 +302,8 @@ __global__ void __launch_bounds__(32 * W3, MINB) k3_lanczos_f32(StepArgs a) {
 }
 
 // ------------------------------------------------ 3-D first and final passes
-// One warp per row of a block-table tile (warp w -> row y0 + w), marching the
-// segment's planes with the 16-byte lane vectors of the strip. Neither pass
+// One warp per row of a block-table tile (warp w -> row y0 + w; the final pass
+// splits a tile over two blocks), marching the segment's planes with the 16-byte lane vectors of the strip. Neither pass
 // forms a vector from another one's stencil, so the y-neighbours of a row are
 // simply loaded (L2 hits: the warps of those rows load them as their own) and
 // the z-neighbours come from a register window; the warps of a block never
@@ -475,12 +476,15 @@ static __global__ void __launch_bounds__(32 * BY3) k3_first_f32(StepArgs a) {
 // of a plane (the window row of V_{kv-1} one plane ahead, its rows above and
 // below, the first eight V_q of each sequence and the fields) is issued before
 // the plane's arithmetic.
-static __global__ void __launch_bounds__(32 * BY3, 1) k3_final_f32(StepArgs a) {
+// Two blocks of BY3/2 warps per block-table tile (block 2i + h: rows
+// y0 + h BY3/2 + w), so that a block's 168-register warps fit on one SM.
+constexpr int FH3 = BY3 / 2;
+static __global__ void __launch_bounds__(32 * FH3, 1) k3_final_f32(StepArgs a) {
   constexpr int NB = 8;
   __shared__ float Wsh[2][KMAX];
   __shared__ float Lsh[2];
-  if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
-  const TileDesc t = a.tiles[blockIdx.x];
+  if ((int)(blockIdx.x >> 1) >= *a.ntiles) return;  // block-uniform
+  const TileDesc t = a.tiles[blockIdx.x >> 1];
   const SlotDesc &s = a.slots[t.slot];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int kv = a.kv;
@@ -491,7 +495,7 @@ static __global__ void __launch_bounds__(32 * BY3, 1) k3_final_f32(StepArgs a) {
     if (lane == 0) Lsh[sq] = F.lam32[0];
   }
   __syncthreads();
-  const int nx = s.nx, ny = s.ny, nz = s.nz, y = t.y0 + w;
+  const int nx = s.nx, ny = s.ny, nz = s.nz, y = t.y0 + (int)(blockIdx.x & 1) * FH3 + w;
   if (y >= ny) return;  // warp-uniform; no barrier follows
   const int step = a.state[t.slot].step;
   const Strip3 S = make_strip3(nx, t.x0, lane);
