@@ -148,6 +148,23 @@ cudaError_t launch2_lanczos1_f32c(const StepArgs &a, int tiles, cudaStream_t st)
     k2_lanczos1_f32c<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
+// Packed complex64 pass (NLSE, c == 1); NLS_C32=0 selects the generic
+// one-sequence complex pass, NLS_C32=3 the build for three blocks per SM.
+int c32_mode() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_C32");
+    const int m = e ? std::atoi(e) : 4;
+    return (m == 0 || m == 3) ? m : 4;
+  }();
+  return v;
+}
+cudaError_t launch2_lanczos1_c32(const StepArgs &a, int tiles, cudaStream_t st) {
+  if (c32_mode() == 3)
+    k2_lanczos1_c32<3><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  else
+    k2_lanczos1_c32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
 cudaError_t launch2_lanczos1_f32c_lo(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_lanczos1_f32c<4, true><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
@@ -393,6 +410,10 @@ template <typename E> KSet make_cplx2() {
   k.sewi_b.lanczos[1] = launch2_lanczos1<E, true>;
   k.sewi_b.final_[0] = launch2_final<E, 1, FIN_SEWI_B, false>;
   k.sewi_b.final_[1] = launch2_final<E, 1, FIN_SEWI_B, true>;
+  if constexpr (std::is_same<E, Cx<float>>::value) {
+    if (c32_mode() != 0)
+      k.ss2.lanczos[0] = k.sewi_a.lanczos[0] = k.sewi_b.lanczos[0] = launch2_lanczos1_c32;
+  }
   k.ftri = launch_ftri<E>;
   k.ring = launch_ring<E, 1>;
   k.set_attrs = attrs_none;

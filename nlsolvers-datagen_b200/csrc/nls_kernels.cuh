@@ -967,6 +967,7 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
 
 #include "nls_kernels_tail.cuh"
 #include "nls_warp2d.cuh"
+#include "nls_warp2d_c32.cuh"
 #include "nls_warp3d.cuh"
 
 }  // namespace nlsb
