@@ -165,6 +165,10 @@ cudaError_t launch2_lanczos1_c32(const StepArgs &a, int tiles, cudaStream_t st) 
     k2_lanczos1_c32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
+cudaError_t launch2_first_c32(const StepArgs &a, int tiles, cudaStream_t st) {
+  k2_first_c32<<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
+  return cudaGetLastError();
+}
 cudaError_t launch2_lanczos1_f32c_lo(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_lanczos1_f32c<4, true><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
@@ -411,8 +415,11 @@ template <typename E> KSet make_cplx2() {
   k.sewi_b.final_[0] = launch2_final<E, 1, FIN_SEWI_B, false>;
   k.sewi_b.final_[1] = launch2_final<E, 1, FIN_SEWI_B, true>;
   if constexpr (std::is_same<E, Cx<float>>::value) {
-    if (c32_mode() != 0)
+    if (c32_mode() != 0) {
       k.ss2.lanczos[0] = k.sewi_a.lanczos[0] = k.sewi_b.lanczos[0] = launch2_lanczos1_c32;
+      k.ss2.first[0] = launch2_first_c32;
+      k.ss2.first_lt[0] = true;
+    }
   }
   k.ftri = launch_ftri<E>;
   k.ring = launch_ring<E, 1>;

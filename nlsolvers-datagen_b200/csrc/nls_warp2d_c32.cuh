@@ -227,3 +227,122 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_c32(StepArgs a) {
     }
   }
 }
+
+// Packed complex64 first pass of the Strang step (SS2, c == 1): one warp per
+// strip of the pass table; x = N_{tau/2}(u) = u exp(i tau/2 rho),
+// rho = (p3 m + q3)|u|^2 (nlse_dev.hpp:20-41), V_0 = x, z = A x and the dots
+// <z, x>, |z|^2, |x|^2 of the first Lanczos step. Raw rows of u and m are
+// prefetched four rows ahead; interior segments run without row masks.
+__device__ __forceinline__ float2 nl_half(float2 u, float m, float half, float p3, float q3) {
+  const float phi = half * ((p3 * m + q3) * (u.x * u.x + u.y * u.y));
+  float sn, cs;
+  sincosf(phi, &sn, &cs);
+  return make_float2(u.x * cs - u.y * sn, u.x * sn + u.y * cs);
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void first_c32_march(const float *pU, const float *pM, float *pV, int P, int PM, int r0,
+                                                int r1, int ny, bool ld, bool io, const SlotDesc &s, const F4 &OPx,
+                                                const F4 &xmiss, double *acc) {
+  // P: row pitch of the complex fields in floats; PM: row pitch of m
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  const float half = float(0.5 * s.dt), p3 = float(s.p3), q3 = float(s.q3);
+  auto ok = [&](int r) { return EDGE ? (ld && r >= 0 && r < ny && r <= r1) : (ld && r <= r1); };
+  auto rowU = [&](int r) -> F4 { return ok(r) ? f4_load(pU + (long long)r * P) : zero4; };
+  auto rowM = [&](int r) -> float2 {
+    return ok(r) ? __ldg(reinterpret_cast<const float2 *>(pM + (long long)r * PM)) : f2(0.f);
+  };
+  auto make = [&](const F4 &u, float2 m) -> F4 {
+    return F4{nl_half(u.a, m.x, half, p3, q3), nl_half(u.b, m.y, half, p3, q3)};
+  };
+  float2 d2r = f2(0.f), d2i = f2(0.f), n1 = f2(0.f), n2 = f2(0.f);
+  F4 X0 = make(rowU(r0 - 1), rowM(r0 - 1)), X1 = make(rowU(r0), rowM(r0)), X2 = zero4, X3 = zero4;
+  F4 U0 = rowU(r0 + 1), U1 = rowU(r0 + 2), U2 = rowU(r0 + 3), U3 = rowU(r0 + 4);
+  float2 M0 = rowM(r0 + 1), M1 = rowM(r0 + 2), M2 = rowM(r0 + 3), M3 = rowM(r0 + 4);
+  const int nit = (r1 - r0 + 3) / 4 * 4;
+#define NLSB_FIRSTC(Xm, Xc, Xp, Uc, Mc)                                                    \
+  {                                                                                        \
+    const int c = r0 + it;                                                                 \
+    Xp = make(Uc, Mc);                                                                     \
+    Uc = rowU(c + 5);                                                                      \
+    Mc = rowM(c + 5);                                                                      \
+    const float2 lft = make_float2(__shfl_up_sync(0xffffffffu, Xc.b.x, 1),                 \
+                                   __shfl_up_sync(0xffffffffu, Xc.b.y, 1));                \
+    const float2 rgt = make_float2(__shfl_down_sync(0xffffffffu, Xc.a.x, 1),               \
+                                   __shfl_down_sync(0xffffffffu, Xc.a.y, 1));              \
+    if (c < r1) {                                                                          \
+      F4 miss = xmiss;                                                                     \
+      if (EDGE) {                                                                          \
+        const float2 rm = f2(float((c == 0) + (c == ny - 1)));                             \
+        miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                   \
+      }                                                                                    \
+      F4 z = lapc(Xm, Xc, Xp, lft, rgt, miss);                                             \
+      z.a = mul2(z.a, OPx.a);                                                              \
+      z.b = mul2(z.b, OPx.b);                                                              \
+      if (io) f4_store(pV + (long long)c * P, Xc);                                         \
+      d2r = fma2(z.a, Xc.a, fma2(z.b, Xc.b, d2r));                                         \
+      d2i = fma2(z.a, swp(Xc.a), fma2(z.b, swp(Xc.b), d2i));                               \
+      n1 = fma2(z.a, z.a, fma2(z.b, z.b, n1));                                             \
+      n2 = fma2(Xc.a, Xc.a, fma2(Xc.b, Xc.b, n2));                                         \
+    }                                                                                      \
+  }
+  for (int it0 = 0; it0 < nit; it0 += 4) {
+    int it = it0;
+    NLSB_FIRSTC(X0, X1, X2, U0, M0) ++it;
+    NLSB_FIRSTC(X1, X2, X3, U1, M1) ++it;
+    NLSB_FIRSTC(X2, X3, X0, U2, M2) ++it;
+    NLSB_FIRSTC(X3, X0, X1, U3, M3)
+    acc[2] += (double)(d2r.x + d2r.y);
+    acc[3] += (double)(d2i.x + d2i.y);
+    acc[6] += (double)(n1.x + n1.y);
+    acc[7] += (double)(n2.x + n2.y);
+    d2r = d2i = n1 = n2 = f2(0.f);
+  }
+#undef NLSB_FIRSTC
+}
+
+static __global__ void __launch_bounds__(32 * WPB) k2_first_c32(StepArgs a) {
+  using E = Cx<float>;
+  WARP_TILE_PROLOGUE
+  const int sq = t.local & 1;
+  const float opsc = float(a.op_sign * s.inv_h2);
+  F4 OPx, xmiss;
+  {
+    float v[2], m[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int x = S.col0 + e;
+      v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
+      m[e] = float((x == 0) + (x == S.nx - 1));
+    }
+    OPx = F4{f2(v[0] * opsc), f2(v[1] * opsc)};
+    xmiss = F4{f2(m[0]), f2(m[1])};
+  }
+  const float *pU = (const float *)a.f.u_hi + 2 * (s.off + S.col0);
+  const float *pM = (const float *)a.f.m + s.off + S.col0;
+  float *pV = (float *)a.V + 2 * ((long long)(sq * a.kv) * a.vstride + s.off + S.col0);
+  const bool ld = S.lane_in, io = S.out_lane;
+  const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = 2 * s.pitch, PM = s.pitch;
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (r0 >= 2 && r1 <= ny - 2)
+    first_c32_march<false>(pU, pM, pV, P, PM, r0, r1, ny, ld, io, s, OPx, xmiss, acc);
+  else
+    first_c32_march<true>(pU, pM, pV, P, PM, r0, r1, ny, ld, io, s, OPx, xmiss, acc);
+  constexpr int ND = 9;
+  double vals[ND];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
+  const int tc = s.tile_count, TT = *a.lt_stride;
+  if (warp_publish<ND>(vals, a.part, wt, a.ticket + t.slot * 2 + sq, tc, lane)) {
+    const double tot = warp_slot_total<ND>(a.part, sq * TT + s.tile_begin, tc, lane);
+    double tv[ND];
+#pragma unroll
+    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
+    if (lane == 0) {
+      double b0;
+      a.scal[(t.slot * 2 + sq) * KMAX + 0] = lz_first<true>(tv, Eps<float>::v, b0);
+      a.beta0[t.slot * 2 + sq] = b0;
+      a.ticket[t.slot * 2 + sq] = 0;
+    }
+  }
+}
