@@ -133,6 +133,29 @@ int nls_pool_poll(nls_pool *pool, int32_t slot, int32_t *steps_done, int32_t *fi
    computed on the device from the FP64 snapshot (m, c as stored: FP32 in an
    FP32 pool) and copied with the snapshot; complete when the snapshot is. */
 int nls_pool_set_diagnostics(nls_pool *pool, int32_t slot, double *diag_dst);
+/* Downsample every snapshot of the slot on the device before its copy to the
+   host (replaces scripts/downsampling.py:68-103 / :215-257 as the reference's
+   HDF5 aggregation applies them to every snapshot,
+   scripts/aggregate_single.py:61-76). Linear interpolation from the grid
+   linspace(-L, L, n) of each array axis onto linspace(-L, L, target), with the
+   array axes (ny, nx) or (nz, ny, nx) paired with (Lx, Ly[, Lz]) in that order,
+   as the aggregation passes them; results equal scipy's
+   RegularGridInterpolator(method='linear') bitwise. target: 2 or 3 extents in
+   array-axis order. traj_dst receives ns downsampled snapshots (NLSE:
+   complex128), vel_dst (KG / phi4, may be NULL) the velocities; both stay valid
+   until release. Call once, after admission and before the slot's first step;
+   from then on the slot's full-size outputs hold snapshot 0 only. */
+int nls_pool_set_downsample(nls_pool *pool, int32_t slot, const int32_t *target, double *traj_dst,
+                            double *vel_dst);
+/* The same interpolation on host arrays, a drop-in for the reference's
+   downsample_interpolation(u, target_shape, Lx, Ly) and
+   downsample_interpolation_3d(u, target_shape, Lx, Ly, Lz)
+   (scripts/downsampling.py:68-103, :215-257): in holds `frames` C-order arrays
+   of shape[0..dim-1] (complex128 when is_complex), out receives `frames`
+   arrays of target[0..dim-1]; half_widths = (Lx, Ly[, Lz]) per array axis.
+   Computed on the current device (synchronous). */
+int nls_downsample_linear(int32_t dim, const int64_t *shape, const int64_t *target, const double *half_widths,
+                          int32_t frames, int32_t is_complex, const double *in, double *out);
 /* Free the slot (waits for its outstanding snapshot copies). */
 int nls_pool_release(nls_pool *pool, int32_t slot);
 /* Wait for all queued device work and copies. */

@@ -18,6 +18,7 @@
 
 #include "../../include/nlsb200.h"
 #include "nls_kernels.cuh"
+#include "nls_downsample.cuh"
 
 using namespace nlsb;
 
@@ -497,6 +498,13 @@ struct SlotHost {
   int ring_cnt = 0;
   double *diag = nullptr;  // ns x 4 diagnostics (host), or null
   bool reg_diag = false;
+  // snapshot downsampling on the device (nls_pool_set_downsample)
+  bool ds = false;
+  DsGeom ds_geom{};
+  int64_t ds_frame = 0;                      // doubles of one downsampled snapshot (all fields)
+  double *ds_traj = nullptr, *ds_vel = nullptr;
+  bool reg_ds_traj = false, reg_ds_vel = false;
+  void *ds_dev = nullptr;                    // tables and staging frame (one allocation)
 };
 
 struct TileSet {
@@ -1088,11 +1096,56 @@ int enqueue_diag(nls_pool *P, int s, int si, int f, cudaStream_t st) {
   return NLS_OK;
 }
 
+// Downsample device frame `frame` (the slot's FP64 snapshot: u, and v for
+// KG / phi4) into the staging frame and copy it to snapshot si of the
+// downsampled outputs, on stream st.
+int enqueue_downsample(nls_pool *P, SlotHost &h, const double *frame, int si, cudaStream_t st) {
+  const DsGeom &g = h.ds_geom;
+  double *stage = (double *)h.ds_dev;
+  const int64_t total = h.ds_frame;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
+  k_downsample<<<blocks, 256, 0, st>>>(g, frame, stage, 1);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h.ds_traj + (int64_t)si * g.dst_field, stage, sizeof(double) * g.dst_field,
+                     cudaMemcpyDeviceToHost, st));
+  if (g.nfields == 2 && h.ds_vel)
+    CK(cudaMemcpyAsync(h.ds_vel + (int64_t)si * g.dst_field, stage + g.dst_field, sizeof(double) * g.dst_field,
+                       cudaMemcpyDeviceToHost, st));
+  return NLS_OK;
+}
+
+// Geometry and device tables of a downsampling from the slot's grid (array
+// axes (ny, nx) or (nz, ny, nx), half-widths (Lx, Ly[, Lz]) in array-axis
+// order, as the reference's aggregation passes them) to `target`.
+int make_ds_tables(int dim, const int64_t *shape, const int64_t *target, const double *L, int comps, int nfields,
+                   DsGeom &g, std::vector<int32_t> &idx, std::vector<double> &y) {
+  g = DsGeom{};
+  g.dim = dim;
+  g.comps = comps;
+  g.nfields = nfields;
+  int64_t np_ = 1, nt_ = 1;
+  for (int d = 0; d < 3; ++d) {
+    g.n[d] = d < dim ? (int)shape[d] : 1;
+    g.t[d] = d < dim ? (int)target[d] : 1;
+    if (d < dim && (shape[d] < 2 || target[d] < 1 || shape[d] > (1 << 24) || target[d] > (1 << 24)))
+      return fail(NLS_ERR_INVALID_ARG, "downsampling needs source extents >= 2 and target extents >= 1");
+    np_ *= g.n[d];
+    nt_ *= g.t[d];
+  }
+  g.src_field = np_ * comps;
+  g.dst_field = nt_ * comps;
+  for (int d = 0; d < dim; ++d) axis_table(L[d], g.n[d], g.t[d], idx, y);
+  return NLS_OK;
+}
+
 int issue_copies(nls_pool *P, SlotHost &h, const SlotDesc &d, int step) {
   if (step % h.freq != 0 || step / h.freq >= h.ns) return NLS_OK;
   const int si = step / h.freq, f = si % NF;
   const double *frame = P->snap + d.snap_off + (int64_t)f * 2 * h.n;
-  if (P->cplx) {
+  if (h.ds) {
+    int rc = enqueue_downsample(P, h, frame, si, P->copy_stream);
+    if (rc) return rc;
+  } else if (P->cplx) {
     CK(cudaMemcpyAsync(h.traj + (int64_t)si * 2 * h.n, frame, sizeof(double) * 2 * h.n,
                        cudaMemcpyDeviceToHost, P->copy_stream));
   } else {
@@ -1561,6 +1614,9 @@ int nls_pool_release(nls_pool *P, int32_t s) {
   if (h.reg_traj) cudaHostUnregister(h.traj);
   if (h.reg_vel) cudaHostUnregister(h.vel);
   if (h.reg_diag) cudaHostUnregister(h.diag);
+  if (h.reg_ds_traj) cudaHostUnregister(h.ds_traj);
+  if (h.reg_ds_vel) cudaHostUnregister(h.ds_vel);
+  if (h.ds_dev) cudaFree(h.ds_dev);
   P->arena.release(h.off, h.npad);
   P->snap_arena.release(h.snap_off, 2 * NF * h.n);
   h = SlotHost();
@@ -1580,6 +1636,84 @@ int nls_pool_set_diagnostics(nls_pool *P, int32_t s, double *diag_dst) {
   std::memset(diag_dst, 0, sizeof(double) * 4 * h.ns);
   // snapshot 0: the input state, written into frame 0 at admission
   return enqueue_diag(P, s, 0, 0, P->stream);
+}
+
+int nls_pool_set_downsample(nls_pool *P, int32_t s, const int32_t *target, double *traj_dst, double *vel_dst) {
+  if (!P || !target || !traj_dst) return fail(NLS_ERR_INVALID_ARG, "null argument");
+  if (s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
+  SlotHost &h = P->hs[s];
+  if (h.step != 1 || h.ds) return fail(NLS_ERR_STATE, "downsampling must be set once, before the slot's first step");
+  const nls_problem &p = h.prob;
+  const int dim = p.dim;
+  const int64_t shape[3] = {dim == 3 ? p.nz : p.ny, dim == 3 ? p.ny : p.nx, dim == 3 ? p.nx : 1};
+  const int64_t tgt[3] = {target[0], target[1], dim == 3 ? target[2] : 1};
+  const double L[3] = {p.Lx, p.Ly, p.Lz};
+  std::vector<int32_t> idx;
+  std::vector<double> y;
+  DsGeom g;
+  const int comps = P->cplx ? 2 : 1, nfields = P->cplx ? 1 : 2;
+  int rc = make_ds_tables(dim, shape, tgt, L, comps, nfields, g, idx, y);
+  if (rc) return rc;
+  // one allocation: staging frame (all fields), distances, indices
+  const size_t stage_b = sizeof(double) * (size_t)(g.dst_field * nfields);
+  const size_t y_b = sizeof(double) * y.size(), i_b = sizeof(int32_t) * idx.size();
+  char *dev = nullptr;
+  CK(cudaMalloc((void **)&dev, stage_b + y_b + i_b));
+  double *dy = (double *)(dev + stage_b);
+  int32_t *di = (int32_t *)(dev + stage_b + y_b);
+  CK(cudaMemcpyAsync(dy, y.data(), y_b, cudaMemcpyHostToDevice, P->stream));
+  CK(cudaMemcpyAsync(di, idx.data(), i_b, cudaMemcpyHostToDevice, P->stream));
+  g.y = dy;
+  g.idx = di;
+  h.ds = true;
+  h.ds_geom = g;
+  h.ds_frame = g.dst_field * nfields;
+  h.ds_dev = dev;
+  h.ds_traj = traj_dst;
+  h.ds_vel = P->cplx ? nullptr : vel_dst;
+  const size_t tb = sizeof(double) * (size_t)g.dst_field * (size_t)h.ns;
+  h.reg_ds_traj = cudaHostRegister(traj_dst, tb, cudaHostRegisterDefault) == cudaSuccess;
+  if (h.ds_vel) h.reg_ds_vel = cudaHostRegister(h.ds_vel, tb, cudaHostRegisterDefault) == cudaSuccess;
+  cudaGetLastError();  // a failed registration (already page-locked) only makes the copies synchronous
+  // snapshot 0: the input state, written into frame 0 at admission
+  const double *frame0 = P->snap + P->sd[s].snap_off;
+  rc = enqueue_downsample(P, h, frame0, 0, P->stream);
+  if (rc) return rc;
+  return NLS_OK;
+}
+
+int nls_downsample_linear(int32_t dim, const int64_t *shape, const int64_t *target, const double *half_widths,
+                          int32_t frames, int32_t is_complex, const double *in, double *out) {
+  if (!shape || !target || !half_widths || !in || !out || (dim != 2 && dim != 3) || frames < 0)
+    return fail(NLS_ERR_INVALID_ARG, "bad downsampling arguments");
+  std::vector<int32_t> idx;
+  std::vector<double> y;
+  DsGeom g;
+  int rc = make_ds_tables(dim, shape, target, half_widths, is_complex ? 2 : 1, 1, g, idx, y);
+  if (rc) return rc;
+  if (frames == 0) return NLS_OK;
+  const size_t in_b = sizeof(double) * (size_t)(g.src_field * frames);
+  const size_t out_b = sizeof(double) * (size_t)(g.dst_field * frames);
+  const size_t y_b = sizeof(double) * y.size(), i_b = sizeof(int32_t) * idx.size();
+  char *dev = nullptr;
+  CK(cudaMalloc((void **)&dev, in_b + out_b + y_b + i_b));
+  double *din = (double *)dev, *dout = (double *)(dev + in_b), *dy = (double *)(dev + in_b + out_b);
+  int32_t *di = (int32_t *)(dev + in_b + out_b + y_b);
+  cudaError_t e = cudaMemcpy(din, in, in_b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dy, y.data(), y_b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(di, idx.data(), i_b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    g.y = dy;
+    g.idx = di;
+    const int64_t total = g.dst_field * frames;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 65536);
+    k_downsample<<<blocks, 256>>>(g, din, dout, frames);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, out_b, cudaMemcpyDeviceToHost);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
+  return NLS_OK;
 }
 
 int nls_set_diagnostics(nls_handle *H, double *diag_dst) {

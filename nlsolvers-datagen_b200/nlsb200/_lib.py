@@ -33,6 +33,7 @@ SYMBOLS = [
     "nls_pool_kernels_per_step", "nls_pool_destroy", "nls_strerror", "nls_last_error",
     "nls_pool_step_timed", "nls_set_device", "nls_host_alloc", "nls_host_free",
     "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
+    "nls_pool_set_downsample", "nls_downsample_linear",
 ]
 
 
@@ -107,6 +108,8 @@ def lib() -> ctypes.CDLL:
         "nls_gautschi_step_noalloc": [pp, vp, vp, vp, vp, i32, i32, vp],
         "nls_pool_set_diagnostics": [vp, i32, dp],
         "nls_set_diagnostics": [vp, dp],
+        "nls_pool_set_downsample": [vp, i32, ip, dp, dp],
+        "nls_downsample_linear": [i32, ctypes.POINTER(i64), ctypes.POINTER(i64), dp, i32, i32, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

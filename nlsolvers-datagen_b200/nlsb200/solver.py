@@ -111,6 +111,36 @@ def pinned_empty(shape, dtype=np.float64):
     return np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
 
 
+def _downsample(u, target_shape, L):
+    u = np.asarray(u)
+    cplx = np.iscomplexobj(u)
+    dim = u.ndim - 1
+    tgt = tuple(int(t) for t in target_shape)
+    src = np.ascontiguousarray(u, dtype=np.complex128 if cplx else np.float64)
+    out = np.empty((u.shape[0],) + tgt, dtype=src.dtype)
+    shape = (ctypes.c_int64 * 3)(*u.shape[1:])
+    tg = (ctypes.c_int64 * 3)(*tgt)
+    hw = (ctypes.c_double * 3)(*[float(x) for x in L])
+    check(lib().nls_downsample_linear(dim, shape, tg, hw, u.shape[0], int(cplx), _dptr(src.view(np.float64)),
+                                      _dptr(out.view(np.float64))))
+    return out.astype(u.dtype)
+
+
+def downsample_interpolation(u, target_shape, Lx, Ly):
+    """Drop-in for the reference's downsample_interpolation
+    (scripts/downsampling.py:68-103): u (frames, n0, n1) onto linspace grids of
+    target_shape, computed on the GPU; equal to it bitwise."""
+    assert np.ndim(u) == 3 and len(target_shape) == 2
+    return _downsample(u, target_shape, (Lx, Ly))
+
+
+def downsample_interpolation_3d(u, target_shape, Lx, Ly, Lz):
+    """Drop-in for the reference's downsample_interpolation_3d
+    (scripts/downsampling.py:215-257): u (frames, n0, n1, n2)."""
+    assert np.ndim(u) == 4 and len(target_shape) == 3
+    return _downsample(u, target_shape, (Lx, Ly, Lz))
+
+
 def _dptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -194,6 +224,8 @@ class SlotInfo:
     vel: np.ndarray | None
     inputs: tuple = field(default_factory=tuple)
     diag: np.ndarray | None = None
+    ds_traj: np.ndarray | None = None   # downsampled snapshots (set_downsample)
+    ds_vel: np.ndarray | None = None
 
 
 class Pool:
@@ -242,6 +274,25 @@ class Pool:
         info.diag = np.zeros((info.spec.ns, 4))
         check(lib().nls_pool_set_diagnostics(self._p, slot, _dptr(info.diag)))
         return info.diag
+
+    def set_downsample(self, slot: int, target_shape):
+        """Downsample every snapshot of `slot` on the device to `target_shape`
+        (array-axis order) before its copy to the host, as the reference's HDF5
+        aggregation does on the host (see nls_pool_set_downsample). Call before
+        the slot's first step; returns (ds_traj, ds_vel) of shape
+        (ns,) + target_shape, filled as snapshots complete (ds_vel is None for
+        the NLSE); the slot's full-size outputs then hold snapshot 0 only."""
+        info = self.slots[slot]
+        spec = info.spec
+        tgt = tuple(int(t) for t in target_shape)
+        if len(tgt) != spec.dim:
+            raise ValueError(f"target shape {tgt} does not match a {spec.dim}-D slot")
+        traj = np.zeros((spec.ns,) + tgt, dtype=np.complex128 if spec.complex else np.float64)
+        vel = None if spec.complex else np.zeros((spec.ns,) + tgt)
+        t32 = (ctypes.c_int32 * 3)(*(tgt + (1,) * (3 - len(tgt))))
+        check(lib().nls_pool_set_downsample(self._p, slot, t32, _dptr(traj.view(np.float64)), _dptr(vel)))
+        info.ds_traj, info.ds_vel = traj, vel
+        return traj, vel
 
     def step(self, nsteps: int = 1):
         check(lib().nls_pool_step(self._p, int(nsteps)))
