@@ -120,6 +120,11 @@ int nls_pool_step(nls_pool *pool, int32_t nsteps);
 /* steps_done: completed steps; finished: 1 when all steps ran and every
    snapshot has reached the host buffers. */
 int nls_pool_poll(nls_pool *pool, int32_t slot, int32_t *steps_done, int32_t *finished);
+/* count: how many leading snapshots (0 .. count-1) are complete in the host
+   buffers (the full-size or the downsampled ones), so that a caller can stream
+   them to files while later steps run (the reference's drivers write their
+   .npy outputs only at the end, kg_driver_dev_2d.cpp:156-158). */
+int nls_pool_snapshots_ready(nls_pool *pool, int32_t slot, int32_t *count);
 /* Per-snapshot energy and mass (the reference computes them post hoc from the
    snapshots: scripts/compare_utils_real_2d.py:112-131,
    scripts/compare_utils_complex_2d.py:134-151). Call once, after admission and

@@ -505,6 +505,9 @@ struct SlotHost {
   double *ds_traj = nullptr, *ds_vel = nullptr;
   bool reg_ds_traj = false, reg_ds_vel = false;
   void *ds_dev = nullptr;                    // tables and staging frame (one allocation)
+  // completion of each snapshot's copies (snapshot si >= 1), for nls_pool_snapshots_ready
+  std::vector<cudaEvent_t> snap_ev;
+  int snaps_ready = 1;
 };
 
 struct TileSet {
@@ -1161,6 +1164,9 @@ int issue_copies(nls_pool *P, SlotHost &h, const SlotDesc &d, int step) {
   }
   CK(cudaEventRecord(h.copy_done[f], P->copy_stream));
   h.copy_pending[f] = true;
+  if ((int)h.snap_ev.size() < h.ns) h.snap_ev.resize((size_t)h.ns, nullptr);
+  if (!h.snap_ev[(size_t)si]) CK(cudaEventCreateWithFlags(&h.snap_ev[(size_t)si], cudaEventDisableTiming));
+  CK(cudaEventRecord(h.snap_ev[(size_t)si], P->copy_stream));
   return NLS_OK;
 }
 
@@ -1602,6 +1608,24 @@ int nls_pool_poll(nls_pool *P, int32_t s, int32_t *steps_done, int32_t *finished
   return NLS_OK;
 }
 
+int nls_pool_snapshots_ready(nls_pool *P, int32_t s, int32_t *count) {
+  if (!P || !count || s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
+  SlotHost &h = P->hs[s];
+  // snapshot 0 is in the host buffers from admission; snapshot si >= 1 was
+  // issued when step si * freq was enqueued, and its copies end with snap_ev[si]
+  const int issued = std::min(h.ns, (h.step - 1) / h.freq + 1);
+  while (h.snaps_ready < issued) {
+    cudaEvent_t ev = h.snaps_ready < (int)h.snap_ev.size() ? h.snap_ev[(size_t)h.snaps_ready] : nullptr;
+    if (!ev) break;
+    const cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaErrorNotReady) break;
+    if (e != cudaSuccess) return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
+    ++h.snaps_ready;
+  }
+  *count = h.snaps_ready;
+  return NLS_OK;
+}
+
 int nls_pool_release(nls_pool *P, int32_t s) {
   if (!P || s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
   SlotHost &h = P->hs[s];
@@ -1617,6 +1641,8 @@ int nls_pool_release(nls_pool *P, int32_t s) {
   if (h.reg_ds_traj) cudaHostUnregister(h.ds_traj);
   if (h.reg_ds_vel) cudaHostUnregister(h.ds_vel);
   if (h.ds_dev) cudaFree(h.ds_dev);
+  for (cudaEvent_t ev : h.snap_ev)
+    if (ev) cudaEventDestroy(ev);
   P->arena.release(h.off, h.npad);
   P->snap_arena.release(h.snap_off, 2 * NF * h.n);
   h = SlotHost();
@@ -1844,6 +1870,12 @@ int nls_pool_destroy(nls_pool *P) {
       if (h.copy_done[f]) cudaEventDestroy(h.copy_done[f]);
     if (h.reg_traj) cudaHostUnregister(h.traj);
     if (h.reg_vel) cudaHostUnregister(h.vel);
+    if (h.reg_diag) cudaHostUnregister(h.diag);
+    if (h.reg_ds_traj) cudaHostUnregister(h.ds_traj);
+    if (h.reg_ds_vel) cudaHostUnregister(h.ds_vel);
+    if (h.ds_dev) cudaFree(h.ds_dev);
+    for (cudaEvent_t ev : h.snap_ev)
+      if (ev) cudaEventDestroy(ev);
   }
   if (P->gexec) cudaGraphExecDestroy(P->gexec);
   pool_free_device(P);

@@ -15,6 +15,7 @@ Latency of a request = completion time - arrival time (wall clock).
 from __future__ import annotations
 
 import math
+import os
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -85,7 +86,11 @@ class Server:
         for p in self.pools.values():
             p.close()
 
-    def run(self, requests: list[Request], clock=time.perf_counter, timeout_s: float = 600.0) -> ServeStats:
+    def run(self, requests: list[Request], clock=time.perf_counter, timeout_s: float = 600.0,
+            out_dir: str | None = None) -> ServeStats:
+        """Serve `requests`; with out_dir, every request's snapshots are also
+        streamed to out_dir/req<rid>_traj.npy (and _vel.npy for KG / phi^4) as
+        they reach the host, in the reference drivers' .npy layout."""
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         queues = {name: deque() for name in self.classes}
         running = {name: {} for name in self.classes}  # slot -> request
@@ -102,7 +107,11 @@ class Server:
                 pool = self.pools[name]
                 while q:
                     r = q[0]
-                    slot = pool.admit(r.spec, r.u0, r.v0, r.m, r.c)
+                    out = None
+                    if out_dir:
+                        base = os.path.join(out_dir, f"req{r.rid:05d}")
+                        out = (base + "_traj.npy", None if r.spec.complex else base + "_vel.npy")
+                    slot = pool.admit(r.spec, r.u0, r.v0, r.m, r.c, **({"out_npy": out} if out else {}))
                     if slot is None:
                         break  # full: the request waits for a release
                     q.popleft()

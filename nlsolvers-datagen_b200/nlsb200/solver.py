@@ -226,6 +226,9 @@ class SlotInfo:
     diag: np.ndarray | None = None
     ds_traj: np.ndarray | None = None   # downsampled snapshots (set_downsample)
     ds_vel: np.ndarray | None = None
+    out_npy: tuple | None = None        # (traj path, vel path or None): snapshots streamed to .npy
+    streams: list | None = None         # [(memmap, source array)] once streaming started
+    written: int = 0                    # snapshots already in the files
 
 
 class Pool:
@@ -249,14 +252,19 @@ class Pool:
         if segment:
             check(lib().nls_pool_set_segment(self._p, int(segment)))
 
-    def admit(self, spec: Spec, u0, v0, m, c=None, traj=None, vel=None):
-        """Returns the slot id, or None when the pool is full right now."""
+    def admit(self, spec: Spec, u0, v0, m, c=None, traj=None, vel=None, out_npy=None):
+        """Returns the slot id, or None when the pool is full right now.
+
+        out_npy = (traj_path, vel_path or None): the snapshots are also written
+        to these .npy files (the reference drivers' layout: (ns, ny, nx) or
+        (ns, nz, ny, nx), '<f8' or '<c16') as they reach the host, by poll(),
+        stream() and release()."""
         u0, v0, m, c, has_c = _prep(spec, u0, v0, m, c)
+        dt = np.complex128 if spec.complex else np.float64
         if traj is None:
-            traj = np.zeros((spec.ns,) + spec.shape,
-                            dtype=np.complex128 if spec.complex else np.float64)
+            traj = pinned_empty((spec.ns,) + spec.shape, dt) if out_npy else np.zeros((spec.ns,) + spec.shape, dtype=dt)
         if vel is None and not spec.complex:
-            vel = np.zeros((spec.ns,) + spec.shape)
+            vel = pinned_empty((spec.ns,) + spec.shape) if out_npy else np.zeros((spec.ns,) + spec.shape)
         slot = ctypes.c_int32(-1)
         rc = lib().nls_pool_admit(self._p, ctypes.byref(spec.struct(has_c)),
                                   _dptr(u0.view(np.float64)), _dptr(v0), _dptr(m), _dptr(c),
@@ -264,8 +272,35 @@ class Pool:
         if rc == _lib.NLS_ERR_CAPACITY:
             return None
         check(rc)
-        self.slots[slot.value] = SlotInfo(slot.value, spec, traj, vel, (u0, v0, m, c))
+        self.slots[slot.value] = SlotInfo(slot.value, spec, traj, vel, (u0, v0, m, c),
+                                          out_npy=tuple(out_npy) if out_npy else None)
         return slot.value
+
+    def stream(self, slot: int) -> int:
+        """Write the snapshots that reached the host since the last call to the
+        slot's .npy files (admit's out_npy); returns how many are complete."""
+        info = self.slots[slot]
+        n = ctypes.c_int32()
+        check(lib().nls_pool_snapshots_ready(self._p, slot, ctypes.byref(n)))
+        if info.out_npy:
+            self._write_frames(info, n.value)
+        return n.value
+
+    @staticmethod
+    def _write_frames(info, ready):
+        if info.streams is None:
+            src = [info.ds_traj if info.ds_traj is not None else info.traj,
+                   info.ds_vel if info.ds_traj is not None else info.vel]
+            info.streams = []
+            for path, a in zip(info.out_npy, src):
+                if path is not None and a is not None:
+                    mm = np.lib.format.open_memmap(path, mode="w+", dtype=a.dtype, shape=a.shape)
+                    info.streams.append((mm, a))
+        if ready > info.written:
+            for mm, a in info.streams:
+                mm[info.written:ready] = a[info.written:ready]
+                mm.flush()
+            info.written = ready
 
     def enable_diagnostics(self, slot: int):
         """Per-snapshot energy / mass of `slot` (ns x 4; see
@@ -306,11 +341,17 @@ class Pool:
     def poll(self, slot: int):
         done, fin = ctypes.c_int32(), ctypes.c_int32()
         check(lib().nls_pool_poll(self._p, slot, ctypes.byref(done), ctypes.byref(fin)))
+        if self.slots[slot].out_npy:
+            self.stream(slot)
         return done.value, bool(fin.value)
 
     def release(self, slot: int) -> SlotInfo:
         check(lib().nls_pool_release(self._p, slot))
-        return self.slots.pop(slot)
+        info = self.slots.pop(slot)
+        if info.out_npy:
+            self._write_frames(info, info.spec.ns)  # every copy completed in release
+            info.streams = None  # closes the memmaps
+        return info
 
     def sync(self):
         check(lib().nls_pool_sync(self._p))
