@@ -57,6 +57,27 @@ extern "C" {
  * NLSE density rho = (p3 m + q3)|u|^2 (reference: p3 = 1).
  * xi ~ N(0,1) per (seed, step, point) from Philox4x32-10 + Box-Muller.
  */
+/* Nonlinearity kinds. NLS_NL_POLY is the reference's form for every method:
+     KG / phi4: g(u) = (p1 m + q1) u + (p3 m + q3) u^3 (+ (rm m + r0) xi)
+     NLSE:      rho  = (p3 m + q3) |u|^2, N_h(u) = u exp(i h rho)
+   The others have no solver in the reference; its build names them
+   (device/CMakeLists.txt:7-29, sources absent) and its sampler defines the
+   potentials (scripts/real_sampler.py:32-46):
+     NLS_NL_SINE   sine-Gordon:            g(u) = (p1 m + q1) sin u          (+ noise)
+     NLS_NL_DSINE  double sine-Gordon:     g(u) = (p1 m + q1)(sin u + 0.3 sin 2u)
+     NLS_NL_SINH   hyperbolic sine-Gordon: g(u) = (p1 m + q1) sinh u
+     NLS_NL_CQ     cubic-quintic NLSE:     rho = (p3 m + q3)|u|^2 + (rm m + r0)|u|^4
+     NLS_NL_SAT    saturable NLSE:         rho = (p3 m + q3)|u|^2 / (1 + |u|^2)
+   The first three apply to the KG / phi4 methods, the last two to the NLSE. */
+enum {
+  NLS_NL_POLY = 0,
+  NLS_NL_SINE = 1,
+  NLS_NL_DSINE = 2,
+  NLS_NL_SINH = 3,
+  NLS_NL_CQ = 4,
+  NLS_NL_SAT = 5
+};
+
 typedef struct nls_problem {
   int32_t dim;          /* 2 or 3 */
   int32_t nx, ny, nz;   /* grid incl. ghost ring; nz ignored in 2-D */
@@ -68,7 +89,7 @@ typedef struct nls_problem {
   int32_t precision;    /* NLS_FP32 or NLS_FP64 */
   int32_t sewi_variant; /* 0: the reference's operand order, 1: corrected */
   int32_t has_c;        /* 0: c == 1 (c pointer may be NULL) */
-  int32_t reserved;
+  int32_t nonlinearity; /* NLS_NL_*: 0 the reference's forms (below) */
   double p1, q1, p3, q3, rm, r0;
   uint64_t seed;
 } nls_problem;

@@ -98,6 +98,32 @@ template <typename R> __device__ __forceinline__ void comp_add(Cx<R> &hi, Cx<R> 
   comp_add(hi.y, lo.y, inc.y);
 }
 
+// ------------------------------------------------------------ nonlinearities
+// Kinds of the force g(u) (KG / phi^4 family) and of the NLSE density rho;
+// 0 is the reference's own form. The others are the potentials of the
+// reference's sampler (scripts/real_sampler.py:32-46: sin u, sin u + 0.3 sin 2u,
+// sinh u) and the cubic-quintic and saturable NLSE its build names
+// (device/CMakeLists.txt:7-29) without sources.
+enum NlKind { NL_POLY = 0, NL_SINE = 1, NL_DSINE = 2, NL_SINH = 3, NL_CQ = 4, NL_SAT = 5 };
+
+// g(u) without the noise term: (p1 m + q1) u + (p3 m + q3) u^3, or
+// (p1 m + q1) N(u) with N = sin u, sin u + 0.3 sin 2u, sinh u.
+template <typename R> __device__ __forceinline__ R kg_force(int kind, R u, R m, const SlotDesc &s) {
+  if (kind == NL_POLY) return (R(s.p1) * m + R(s.q1)) * u + (R(s.p3) * m + R(s.q3)) * (u * u * u);
+  const R a = R(s.p1) * m + R(s.q1);
+  if (kind == NL_SINE) return a * sin(u);
+  if (kind == NL_DSINE) return a * (sin(u) + R(0.3) * sin(R(2) * u));
+  return a * sinh(u);
+}
+// rho(|u|^2): (p3 m + q3) s (cubic), + (rm m + r0) s^2 (cubic-quintic), or
+// (p3 m + q3) s / (1 + s) (saturable).
+template <typename R> __device__ __forceinline__ R nlse_rho(int kind, R s2, R m, const SlotDesc &s) {
+  const R k3 = R(s.p3) * m + R(s.q3);
+  if (kind == NL_CQ) return k3 * s2 + (R(s.rm) * m + R(s.r0)) * (s2 * s2);
+  if (kind == NL_SAT) return k3 * s2 / (R(1) + s2);
+  return k3 * s2;
+}
+
 // -------------------------------------------------------------- Philox
 // Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), key = seed, counter =
 // (point, step, 0, 0); Box-Muller on two 23-bit uniforms in (0, 1), which are

@@ -612,6 +612,13 @@ int check_problem(const nls_problem *p) {
   if (p->precision != NLS_FP32 && p->precision != NLS_FP64)
     return fail(NLS_ERR_INVALID_ARG, "precision must be NLS_FP32 or NLS_FP64");
   if (!(p->T > 0.0)) return fail(NLS_ERR_INVALID_ARG, "T must be positive");
+  {
+    const bool cplx = p->method == NLS_NLSE_SS2 || p->method == NLS_NLSE_SEWI;
+    const int nk = p->nonlinearity;
+    const bool ok = nk == NLS_NL_POLY || (!cplx && (nk == NLS_NL_SINE || nk == NLS_NL_DSINE || nk == NLS_NL_SINH)) ||
+                    (cplx && (nk == NLS_NL_CQ || nk == NLS_NL_SAT));
+    if (!ok) return fail(NLS_ERR_INVALID_ARG, "nonlinearity kind does not apply to this method");
+  }
   const int64_t n = grid_points(*p);
   if (n > (int64_t)1 << 31) return fail(NLS_ERR_INVALID_ARG, "grid too large (> 2^31 points)");
   return NLS_OK;
@@ -1520,6 +1527,7 @@ int nls_pool_admit(nls_pool *P, const nls_problem *p, const double *u0, const do
   d.off = off;
   d.inv_h2 = p->dim == 2 ? 1.0 / (dx * dy) : 1.0 / (dx * dx);
   d.dt = p->T / p->nt;
+  d.nl_kind = p->nonlinearity;
   d.p1 = p->p1;
   d.q1 = p->q1;
   d.p3 = p->p3;

@@ -201,7 +201,7 @@ template <typename R> struct Src<SRC_KG, R> {
     const R u = ((const R *)a.f.u_hi)[e];
     if (seq == 0) return u;
     const R m = ((const R *)a.f.m)[e];
-    R g = (R(s.p1) * m + R(s.q1)) * u + (R(s.p3) * m + R(s.q3)) * (u * u * u);
+    R g = kg_force<R>(s.nl_kind, u, m, s);
     if (s.rm != 0.0 || s.r0 != 0.0)
       g += (R(s.rm) * m + R(s.r0)) * philox_normal<R>(s.seed, (uint32_t)step, (uint32_t)pt);
     return g;
@@ -213,7 +213,7 @@ template <typename R> struct Src<SRC_SS2, Cx<R>> {
                                                long long e, long long) {
     const Cx<R> u = ((const Cx<R> *)a.f.u_hi)[e];
     const R m = ((const R *)a.f.m)[e];
-    const R phi = R(0.5 * s.dt) * ((R(s.p3) * m + R(s.q3)) * norm2(u));
+    const R phi = R(0.5 * s.dt) * nlse_rho<R>(s.nl_kind, norm2(u), m, s);
     R sn, cs;
     sincos_r(phi, sn, cs);
     return Cx<R>{u.x * cs - u.y * sn, u.x * sn + u.y * cs};
@@ -227,7 +227,7 @@ template <typename R> struct Src<SRC_SEWI_A, Cx<R>> {
     if (seq == 1) return ((const Cx<R> *)a.f.up_hi)[e];
     const Cx<R> u = ((const Cx<R> *)a.f.u_hi)[e];
     const R m = ((const R *)a.f.m)[e];
-    const R r = -((R(s.p3) * m + R(s.q3)) * norm2(u));
+    const R r = -nlse_rho<R>(s.nl_kind, norm2(u), m, s);
     return Cx<R>{r * u.x, r * u.y};
   }
 };

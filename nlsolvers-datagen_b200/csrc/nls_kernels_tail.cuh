@@ -55,12 +55,11 @@ template <typename R> struct Fin<FIN_SS2, Cx<R>> {
                                                long long e, long long pt, const Cx<R> *y) {
     Cx<R> *uh = (Cx<R> *)a.f.u_hi, *ul = (Cx<R> *)a.f.u_lo;
     const R m = ((const R *)a.f.m)[e];
-    const R kap = R(s.p3) * m + R(s.q3);
     Cx<R> hi = uh[e], lo = ul[e];
     const R half = R(0.5 * s.dt);
-    const Cx<R> d1 = cexpm1_mul(hi, half * (kap * norm2(hi)));
+    const Cx<R> d1 = cexpm1_mul(hi, half * nlse_rho<R>(s.nl_kind, norm2(hi), m, s));
     const Cx<R> w = add(add(hi, d1), y[0]);
-    const Cx<R> d2 = cexpm1_mul(w, half * (kap * norm2(w)));
+    const Cx<R> d2 = cexpm1_mul(w, half * nlse_rho<R>(s.nl_kind, norm2(w), m, s));
     comp_add(hi, lo, add(add(d1, y[0]), d2));
     uh[e] = hi;
     ul[e] = lo;
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NT) k_sv(StepArgs a) {
       const R lu = stencil<R, R>(c, b, lm, l0, lp, cm, c0, cp, hc, lx, ly, opsc);
       const R u = l0[c.pidx(lx, ly)];
       const R m = ((const R *)a.f.m)[e];
-      R g = (R(s.p1) * m + R(s.q1)) * u + (R(s.p3) * m + R(s.q3)) * (u * u * u);
+      R g = kg_force<R>(s.nl_kind, u, m, s);
       if (noisy) g += (R(s.rm) * m + R(s.r0)) * philox_normal<R>(s.seed, (uint32_t)step, (uint32_t)pt);
       R *ul = (R *)a.f.u_lo, *dd = (R *)a.f.d;
       const R dp = dd[e] + (dt * dt) * (lu + g);

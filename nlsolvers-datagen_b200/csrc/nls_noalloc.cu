@@ -214,6 +214,7 @@ int run(const nls_problem &p, double *u, double *u_past, const double *m, const 
   sd.off = 0;
   sd.inv_h2 = 1.0 / (dx * dy);
   sd.dt = p.T / p.nt;
+  sd.nl_kind = p.nonlinearity;
   sd.p1 = p.p1;
   sd.q1 = p.q1;
   sd.p3 = p.p3;

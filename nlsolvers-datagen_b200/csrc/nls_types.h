@@ -23,7 +23,9 @@ struct SlotDesc {
   int64_t n;                 // nx*ny*nz (unpadded points)
   int32_t active;
   int32_t variant;           // NLSE SEWI operand order: 0 reference, 1 corrected
-  int32_t tile_begin2, tile_count2;  // tiles of the TMA-pipelined 2-D passes
+  int32_t tile_begin2, tile_count2;  // tiles of the block-table passes (2-D TMA, 3-D FP32)
+  int32_t nl_kind;           // nonlinearity (NLS_NL_*: 0 polynomial / cubic)
+  int32_t pad_;
 };
 
 // Mutable per-slot state on the device (advanced by the boundary kernel).

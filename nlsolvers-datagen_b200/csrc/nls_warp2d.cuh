@@ -333,7 +333,7 @@ template <typename R> struct SrcRow<SRC_KG, R> {
 #pragma unroll
     for (int q = 0; q < N; ++q) {
       const R u = w.u.v[q], mm = w.m.v[q];
-      R g = (R(s.p1) * mm + R(s.q1)) * u + (R(s.p3) * mm + R(s.q3)) * (u * u * u);
+      R g = kg_force<R>(s.nl_kind, u, mm, s);
       if (noisy) {
         const int xx = S.col0 + q;
         if (S.row_ok(r) && xx >= 0 && xx < S.nx)
@@ -362,7 +362,7 @@ template <typename R> struct SrcRow<SRC_SS2, Cx<R>> {
 #pragma unroll
     for (int q = 0; q < V16<Cx<R>>::N; ++q) {
       const Cx<R> u = w.u.v[q];
-      const R phi = R(0.5 * s.dt) * ((R(s.p3) * w.m.v[q] + R(s.q3)) * norm2(u));
+      const R phi = R(0.5 * s.dt) * nlse_rho<R>(s.nl_kind, norm2(u), w.m.v[q], s);
       const R sn = sin(phi), cs = cos(phi);
       x[0].v[q] = Cx<R>{u.x * cs - u.y * sn, u.x * sn + u.y * cs};
     }
@@ -384,7 +384,7 @@ template <typename R> struct SrcRow<SRC_SEWI_A, Cx<R>> {
                                               int r, V16<Cx<R>> *x) {
 #pragma unroll
     for (int q = 0; q < V16<Cx<R>>::N; ++q) {
-      const R rr = -((R(s.p3) * w.m.v[q] + R(s.q3)) * norm2(w.u.v[q]));
+      const R rr = -nlse_rho<R>(s.nl_kind, norm2(w.u.v[q]), w.m.v[q], s);
       x[0].v[q] = Cx<R>{rr * w.u.v[q].x, rr * w.u.v[q].y};
     }
     x[1] = w.up;
@@ -680,10 +680,9 @@ template <typename R> struct FinRow<FIN_SS2, Cx<R>> {
     const R half = R(0.5 * s.dt);
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-      const R kap = R(s.p3) * f.m.v[q] + R(s.q3);
-      const Cx<R> d1 = cexpm1_mul(f.hi.v[q], half * (kap * norm2(f.hi.v[q])));
+      const Cx<R> d1 = cexpm1_mul(f.hi.v[q], half * nlse_rho<R>(s.nl_kind, norm2(f.hi.v[q]), f.m.v[q], s));
       const Cx<R> w = add(add(f.hi.v[q], d1), y[0].v[q]);
-      const Cx<R> d2 = cexpm1_mul(w, half * (kap * norm2(w)));
+      const Cx<R> d2 = cexpm1_mul(w, half * nlse_rho<R>(s.nl_kind, norm2(w), f.m.v[q], s));
       comp_add(f.hi.v[q], f.lo.v[q], add(add(d1, y[0].v[q]), d2));
     }
     vmask(f.hi, S, r);
@@ -944,7 +943,7 @@ __global__ void __launch_bounds__(32 * WPB) k2_sv(StepArgs a) {
 #pragma unroll
     for (int q = 0; q < N; ++q) {
       const R u = Uo.v[q], mm = m.v[q];
-      R g = (R(s.p1) * mm + R(s.q1)) * u + (R(s.p3) * mm + R(s.q3)) * (u * u * u);
+      R g = kg_force<R>(s.nl_kind, u, mm, s);
       const int x = S.col0 + q;
       if (noisy && x >= 0 && x < S.nx)
         g += (R(s.rm) * mm + R(s.r0)) *
@@ -1731,6 +1730,13 @@ __device__ __forceinline__ F4 f4_g(const F4 &u, const F4 &m, float2 P1, float2 Q
   const float2 ua3 = mul2(mul2(u.a, u.a), u.a), ub3 = mul2(mul2(u.b, u.b), u.b);
   return F4{fma2(a1, u.a, mul2(a3, ua3)), fma2(b1, u.b, mul2(b3, ub3))};
 }
+// g(u) of any nonlinearity kind on a lane vector (the polynomial in packed form)
+__device__ __forceinline__ F4 f4_force(int kind, const F4 &u, const F4 &m, const SlotDesc &s, float2 P1, float2 Q1,
+                                       float2 P3, float2 Q3) {
+  if (kind == NL_POLY) return f4_g(u, m, P1, Q1, P3, Q3);
+  return F4{make_float2(kg_force<float>(kind, u.a.x, m.a.x, s), kg_force<float>(kind, u.a.y, m.a.y, s)),
+            make_float2(kg_force<float>(kind, u.b.x, m.b.x, s), kg_force<float>(kind, u.b.y, m.b.y, s))};
+}
 
 template <bool EDGE, int SQ>
 __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM, float *pV, int P, int r0, int r1,
@@ -1751,7 +1757,7 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
   // source row r from its raw rows (g and noise for sequence 1; zero outside the grid)
   auto make = [&](const F4 &u, const F4 &m, int r) -> F4 {
     if (SQ == 0) return u;
-    F4 x = f4_g(u, m, P1, Q1, P3, Q3);
+    F4 x = f4_force(s.nl_kind, u, m, s, P1, Q1, P3, Q3);
     if (noisy && r >= 0 && r < ny) {
       float xs[4] = {x.a.x, x.a.y, x.b.x, x.b.y};
       const float ms[4] = {m.a.x, m.a.y, m.b.x, m.b.y};

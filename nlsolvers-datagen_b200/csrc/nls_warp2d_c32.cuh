@@ -230,11 +230,12 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_c32(StepArgs a) {
 
 // Packed complex64 first pass of the Strang step (SS2, c == 1): one warp per
 // strip of the pass table; x = N_{tau/2}(u) = u exp(i tau/2 rho),
-// rho = (p3 m + q3)|u|^2 (nlse_dev.hpp:20-41), V_0 = x, z = A x and the dots
+// rho = (p3 m + q3)|u|^2 (nlse_dev.hpp:20-41; the other kinds as nlse_rho),
+// V_0 = x, z = A x and the dots
 // <z, x>, |z|^2, |x|^2 of the first Lanczos step. Raw rows of u and m are
 // prefetched four rows ahead; interior segments run without row masks.
-__device__ __forceinline__ float2 nl_half(float2 u, float m, float half, float p3, float q3) {
-  const float phi = half * ((p3 * m + q3) * (u.x * u.x + u.y * u.y));
+__device__ __forceinline__ float2 nl_half(float2 u, float m, float half, const SlotDesc &s) {
+  const float phi = half * nlse_rho<float>(s.nl_kind, u.x * u.x + u.y * u.y, m, s);
   float sn, cs;
   sincosf(phi, &sn, &cs);
   return make_float2(u.x * cs - u.y * sn, u.x * sn + u.y * cs);
@@ -246,14 +247,14 @@ __device__ __forceinline__ void first_c32_march(const float *pU, const float *pM
                                                 const F4 &xmiss, double *acc) {
   // P: row pitch of the complex fields in floats; PM: row pitch of m
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
-  const float half = float(0.5 * s.dt), p3 = float(s.p3), q3 = float(s.q3);
+  const float half = float(0.5 * s.dt);
   auto ok = [&](int r) { return EDGE ? (ld && r >= 0 && r < ny && r <= r1) : (ld && r <= r1); };
   auto rowU = [&](int r) -> F4 { return ok(r) ? f4_load(pU + (long long)r * P) : zero4; };
   auto rowM = [&](int r) -> float2 {
     return ok(r) ? __ldg(reinterpret_cast<const float2 *>(pM + (long long)r * PM)) : f2(0.f);
   };
   auto make = [&](const F4 &u, float2 m) -> F4 {
-    return F4{nl_half(u.a, m.x, half, p3, q3), nl_half(u.b, m.y, half, p3, q3)};
+    return F4{nl_half(u.a, m.x, half, s), nl_half(u.b, m.y, half, s)};
   };
   float2 d2r = f2(0.f), d2i = f2(0.f), n1 = f2(0.f), n2 = f2(0.f);
   F4 X0 = make(rowU(r0 - 1), rowM(r0 - 1)), X1 = make(rowU(r0), rowM(r0)), X2 = zero4, X3 = zero4;

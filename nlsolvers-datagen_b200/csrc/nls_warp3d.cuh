@@ -320,7 +320,7 @@ template <int SQ>
 __device__ __forceinline__ F4 src3(const F4 &u, const F4 &m, const SlotDesc &s, int step, int col0, int nx,
                                    long long row_pt, bool noisy, bool ok) {
   if (SQ == 0) return u;
-  F4 x = f4_g(u, m, f2(float(s.p1)), f2(float(s.q1)), f2(float(s.p3)), f2(float(s.q3)));
+  F4 x = f4_force(s.nl_kind, u, m, s, f2(float(s.p1)), f2(float(s.q1)), f2(float(s.p3)), f2(float(s.q3)));
   if (noisy && ok) {
     float xs[4] = {x.a.x, x.a.y, x.b.x, x.b.y};
     const float ms[4] = {m.a.x, m.a.y, m.b.x, m.b.y};

@@ -23,6 +23,8 @@ NLS_ERR_CAPACITY = -6
 NLS_ERR_NO_DEVICE = -5
 
 KG_GAUTSCHI, KG_SV, SP4_SV, SP4_GAUTSCHI, NLSE_SS2, NLSE_SEWI = range(6)
+# nonlinearity kinds (nls_problem.nonlinearity, include/nlsb200.h)
+NL_POLY, NL_SINE, NL_DSINE, NL_SINH, NL_CQ, NL_SAT = range(6)
 FP32, FP64 = 0, 1
 
 SYMBOLS = [
@@ -51,7 +53,7 @@ class Problem(ctypes.Structure):
         ("Lz", ctypes.c_double), ("T", ctypes.c_double), ("nt", ctypes.c_int32),
         ("ns", ctypes.c_int32), ("k", ctypes.c_int32), ("method", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("sewi_variant", ctypes.c_int32),
-        ("has_c", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("has_c", ctypes.c_int32), ("nonlinearity", ctypes.c_int32),
         ("p1", ctypes.c_double), ("q1", ctypes.c_double), ("p3", ctypes.c_double),
         ("q3", ctypes.c_double), ("rm", ctypes.c_double), ("r0", ctypes.c_double),
         ("seed", ctypes.c_uint64),

@@ -15,8 +15,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (FP32, FP64, KG_GAUTSCHI, KG_SV, NLSE_SEWI, NLSE_SS2, SP4_GAUTSCHI, SP4_SV,
-                   NlsError, check, lib)
+from ._lib import (FP32, FP64, KG_GAUTSCHI, KG_SV, NL_CQ, NL_DSINE, NL_POLY, NL_SAT, NL_SINE, NL_SINH,
+                   NLSE_SEWI, NLSE_SS2, SP4_GAUTSCHI, SP4_SV, NlsError, check, lib)
 
 COMPLEX_METHODS = (NLSE_SS2, NLSE_SEWI)
 KRYLOV_METHODS = (KG_GAUTSCHI, SP4_GAUTSCHI, NLSE_SS2, NLSE_SEWI)
@@ -46,6 +46,7 @@ class Spec:
     rm: float | None = None
     r0: float = 0.0
     seed: int = 0
+    nonlinearity: int = 0   # NL_* kind (0: the reference's polynomial / cubic form)
 
     @property
     def shape(self):
@@ -84,12 +85,13 @@ class Spec:
         elif self.method in (SP4_SV, SP4_GAUTSCHI):
             p.rm = reference_phi4_rm(self)
         p.seed = self.seed
+        p.nonlinearity = self.nonlinearity
         return p
 
     def oracle_params(self):
         """Nonlinearity coefficients as the library resolves them."""
         s = self.struct(False)
-        return dict(k=s.k, p1=s.p1, q1=s.q1, p3=s.p3, q3=s.q3, rm=s.rm, r0=s.r0)
+        return dict(k=s.k, p1=s.p1, q1=s.q1, p3=s.p3, q3=s.q3, rm=s.rm, r0=s.r0, nonlinearity=s.nonlinearity)
 
 
 def reference_phi4_rm(spec: Spec) -> float:

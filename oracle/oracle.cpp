@@ -377,8 +377,21 @@ int derive(const orc_problem *p, Derived &D) {
 }
 
 inline double force(const orc_problem *p, double u, double m, double xi) {
-  return (p->p1 * m + p->q1) * u + (p->p3 * m + p->q3) * (u * u * u) +
-         (p->rm * m + p->r0) * xi;
+  const double a = p->p1 * m + p->q1, noise = (p->rm * m + p->r0) * xi;
+  switch (p->nonlinearity) {
+    case 1: return a * std::sin(u) + noise;
+    case 2: return a * (std::sin(u) + 0.3 * std::sin(2.0 * u)) + noise;
+    case 3: return a * std::sinh(u) + noise;
+    default: return a * u + (p->p3 * m + p->q3) * (u * u * u) + noise;
+  }
+}
+
+// NLSE density rho(|u|^2) (nlse_dev.hpp:20-41 for the cubic kind 0)
+inline double nlse_rho(const orc_problem *p, double s2, double m) {
+  const double k3 = p->p3 * m + p->q3;
+  if (p->nonlinearity == 4) return k3 * s2 + (p->rm * m + p->r0) * (s2 * s2);
+  if (p->nonlinearity == 5) return k3 * s2 / (1.0 + s2);
+  return k3 * s2;
 }
 
 // State of a KG / phi4 trajectory between steps (kg_dev.hpp:319-339).
@@ -495,7 +508,7 @@ int run_nlse(const orc_problem *p, const Derived &D, const cd *u0, const double 
     if (cur < p->ns) std::copy(u.begin(), u.end(), traj + (size_t)cur * n);
     if (cur < p->ns) ++cur;
   };
-  auto rho = [&](long i) { return (p->p3 * m[i] + p->q3) * std::norm(u[i]); };
+  auto rho = [&](long i) { return nlse_rho(p, std::norm(u[i]), m[i]); };
   auto ss2 = [&](int step) -> int {
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < n; ++i) buf[i] = u[i] * std::exp(0.5 * tau * cd(rho(i), 0.0));

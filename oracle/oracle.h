@@ -52,9 +52,13 @@ typedef struct orc_problem {
   int32_t sewi_variant; /* 0: reference operand order, 1: corrected */
   int32_t reorth;       /* 1: classical Gram-Schmidt pass as lanczos.hpp:249-250 */
   int32_t max_steps;    /* >0: stop after this many steps (bounded timing sample) */
-  int32_t pad_;
+  int32_t nonlinearity; /* 0: the forms below; 1-3 (KG / phi4) and 4-5 (NLSE) as noted */
   /* nonlinearity g(u) = (p1 m + q1) u + (p3 m + q3) u^3 + (rm m + r0) xi   (KG / phi4)
-     NLSE density rho = (p3 m + q3) |u|^2                                           */
+     NLSE density rho = (p3 m + q3) |u|^2                                           
+     other kinds (no solver in the reference; its sampler defines the potentials,
+     scripts/real_sampler.py:32-46): g = (p1 m + q1) N(u) + (rm m + r0) xi with
+     N = sin u (1), sin u + 0.3 sin 2u (2), sinh u (3); rho = (p3 m + q3)|u|^2 +
+     (rm m + r0)|u|^4 (4, cubic-quintic), (p3 m + q3)|u|^2 / (1 + |u|^2) (5, saturable) */
   double p1, q1, p3, q3, rm, r0;
   uint64_t seed;        /* Philox key for phi4 noise */
 } orc_problem;

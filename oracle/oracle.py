@@ -32,7 +32,7 @@ class _Problem(ctypes.Structure):
         ("Lz", ctypes.c_double), ("T", ctypes.c_double), ("nt", ctypes.c_int32),
         ("ns", ctypes.c_int32), ("k", ctypes.c_int32), ("method", ctypes.c_int32),
         ("sewi_variant", ctypes.c_int32), ("reorth", ctypes.c_int32),
-        ("max_steps", ctypes.c_int32), ("pad_", ctypes.c_int32),
+        ("max_steps", ctypes.c_int32), ("nonlinearity", ctypes.c_int32),
         ("p1", ctypes.c_double), ("q1", ctypes.c_double), ("p3", ctypes.c_double),
         ("q3", ctypes.c_double), ("rm", ctypes.c_double), ("r0", ctypes.c_double),
         ("seed", ctypes.c_uint64),
@@ -188,13 +188,12 @@ class Problem:
     rm: float = 0.0
     r0: float = 0.0
     seed: int = 0
+    nonlinearity: int = 0
     extra: dict = field(default_factory=dict)
 
     def struct(self):
         s = _Problem()
         for name, _ in _Problem._fields_:
-            if name == "pad_":
-                continue
             setattr(s, name, getattr(self, name))
         return s
 

@@ -10,7 +10,8 @@ def oracle_problem(spec, reorth=True, max_steps=0):
                      Lx=spec.Lx, Ly=spec.Ly, Lz=spec.Lz, T=spec.T, nt=spec.nt, ns=spec.ns,
                      k=prm["k"], method=spec.method, sewi_variant=spec.sewi_variant,
                      reorth=int(reorth), max_steps=max_steps, p1=prm["p1"], q1=prm["q1"],
-                     p3=prm["p3"], q3=prm["q3"], rm=prm["rm"], r0=prm["r0"], seed=spec.seed)
+                     p3=prm["p3"], q3=prm["q3"], rm=prm["rm"], r0=prm["r0"], seed=spec.seed,
+                     nonlinearity=prm["nonlinearity"])
 
 
 def run_oracle(spec, u0, v0, m, c, reorth=True):
