@@ -292,7 +292,14 @@ def run_small(args, lrank):
     nl.lib().nls_set_device(lrank)
     B, k = args.batch, 10
     dim = 3 if args.dim3 else 2
-    if dim == 3:
+    method = KG_GAUTSCHI
+    if args.nlse:
+        # NLSE 2-D SS2 boxes of 200^2 on [-10,10]^2, dt = 1e-3, k = 12 (the batched NLSE configuration's shape)
+        from nlsb200.solver import NLSE_SS2
+        method, k = NLSE_SS2, 12
+        cases = [W.nlse_case(200, 10.0, T=2.0, nt=2000, ns=100, k=k, seed=i, precision=FP32) for i in range(B)]
+        cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
+    elif dim == 3:
         # KG 3-D Gautschi boxes of dim3^3 on [-10,10]^3, dt = 0.01, 40 snapshots
         cases = [W.kg_case(args.dim3, 10.0, T=100.0, nt=10000, ns=40, k=k, seed=i, dim=3, precision=FP32)
                  for i in range(B)]
@@ -300,14 +307,14 @@ def run_small(args, lrank):
     else:
         cases = make_batch(B, 0, k)
         cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
-    pool = Pool(KG_GAUTSCHI, dim, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg)
+    pool = Pool(method, dim, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg)
     for cs in cases:
         assert pool.admit(*cs) is not None
     pool.step(args.warmup)
     ms = pool.step_timed(args.steps)
     pool.sync()
     pass_ms, _ = pool.time_pass(2, 20)
-    print(json.dumps({"small": True, "dim": dim, "n": cases[0][0].nx, "batch": B, "k": k, "seg": args.seg,
+    print(json.dumps({"small": True, "method": int(method), "dim": dim, "n": cases[0][0].nx, "batch": B, "k": k, "seg": args.seg,
                       "ms_per_step": ms / args.steps,
                       "pass_ms": pass_ms, "kernels_per_step": pool.kernels_per_step()}), flush=True)
     pool.close()
@@ -451,6 +458,7 @@ def main():
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
     ap.add_argument("--seg", type=int, default=32, help="segment rows (planes in 3-D) of the --small case")
+    ap.add_argument("--nlse", action="store_true", help="--small case as NLSE 2-D SS2 boxes of 200^2 (k = 12)")
     ap.add_argument("--dim3", type=int, default=0,
                     help="--small case as KG 3-D boxes of DIM3^3 points (0: the 2-D 300^2 workload)")
     args = ap.parse_args()
