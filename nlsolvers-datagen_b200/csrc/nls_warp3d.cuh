@@ -19,7 +19,7 @@
 //
 // Plane q of the march forms v_j(q) = (sA L V_{j-1} - a sA V_{j-1} - d sB V_{j-2})(q) / b
 // for q = p0-1 .. p1 and z at plane q-1, as the 2-D rows do.
-constexpr int W3 = 24;         // warps per block
+constexpr int W3 = 20;         // warps per block
 constexpr int BY3 = W3 - 4;    // output rows per block
 constexpr int PD3 = 3;         // planes in flight beyond the three in use
 constexpr int RS3 = PD3 + 3;   // ring slots per warp and vector (the unroll factor of the march)
@@ -84,18 +84,18 @@ __device__ __forceinline__ Strip3 make_strip3(int nx, int x0, int lane) {
   return S;
 }
 
-// The march keeps no plane of V_{j-1} or v_j in registers across planes: the
-// warp re-reads its own rows from its ring and from the v_j buffer, which keeps
-// the register count low enough for one block of 24 warps per SM. The loop is
-// unrolled by the ring length RS3 (a multiple of the buffer length NV3), so
-// every ring and buffer offset is a compile-time constant.
+// Each warp keeps its own rows of V_{j-1} (planes q-1 .. q+1) and v_j (planes
+// q-2 .. q) in registers and reads only its neighbours' rows from shared
+// memory (20 warps of at most 102 registers per SM). The loop is unrolled by the
+// ring length RS3 (a multiple of the window and buffer length 3), so every ring
+// and buffer offset is a compile-time constant.
 template <bool EDGE>
 __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const float *rowA, const float *rowB,
                                              const float *safe, float *rowJ, long long PS, int p0, int p1, int nz,
                                              bool ldA, bool ldB, bool form, bool outw, bool io, float2 CA,
                                              float2 CB, const F4 &CSx, const F4 &OPx, const F4 &miss0,
                                              double *acc) {
-  static_assert(RS3 % NV3 == 0, "unroll by the ring length must cycle the v_j buffer");
+  static_assert(RS3 % NV3 == 0, "unroll by the ring length must cycle the windows and the v_j buffer");
   const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&sm.A[w][0][lane * 16]);
   const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&sm.B[w][0][lane * 16]);
   const uint32_t cellV = (uint32_t)__cvta_generic_to_shared(&sm.V[0][w][lane * 16]);
@@ -124,25 +124,29 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
 #pragma unroll
   for (int f = 0; f < PD3 + 2; ++f) fetch(f, f * 512);
   float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
+  cp_async_wait<PD3>();  // fetches 0, 1 landed (own rows; no other warp reads them yet)
+  const F4 zero4 = F4{f2(0.f), f2(0.f)};
+  F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2 = zero4;
+  F4 V0 = zero4, V1 = zero4, V2 = zero4;
   float *sp = rowJ + (long long)(p0 - 1) * PS;  // row of plane q in V_j
   const int last_it = p1 - p0;                   // iterations 1 .. last_it store V_j, 2 .. last_it+1 reduce
   const int nit = (p1 - p0 + 2 + RS3 - 1) / RS3 * RS3;
-  // iteration it = it0 + K: A planes q-1, q, q+1 in slots K, K+1, K+2 (mod RS3),
-  // B plane q in slot K+1; v_j(q) into buffer plane K % NV3, v_j(q-1) and
-  // v_j(q-2) in planes (K+2) % NV3 and (K+1) % NV3
-#define NLSB_PLANE3(K)                                                                        \
+  // iteration it = it0 + K: A planes q-1, q, q+1 are the window (Am, Ac, Ap),
+  // Ap read from ring slot K+2; the neighbours' rows of plane q and B(q) are in
+  // slot K+1; v_j(q) goes to buffer plane K % NV3 and the neighbours' v_j(q-1)
+  // are read from plane (K+2) % NV3
+#define NLSB_PLANE3(K, Am, Ac, Ap, Vm, Vc, Vn)                                                \
   {                                                                                           \
     const int it = it0 + (K);                                                                 \
     const int q = p0 - 1 + it;                                                                \
-    constexpr uint32_t sm1 = ((K) % RS3) * 512, s0 = (((K) + 1) % RS3) * 512,                 \
-                       sp1 = (((K) + 2) % RS3) * 512, sf = (((K) + PD3 + 2) % RS3) * 512;     \
-    constexpr uint32_t vn = ((K) % NV3) * VPL, vc = (((K) + 2) % NV3) * VPL,                  \
-                       vm = (((K) + 1) % NV3) * VPL;                                          \
+    constexpr uint32_t s0 = (((K) + 1) % RS3) * 512, sp1 = (((K) + 2) % RS3) * 512,           \
+                       sf = (((K) + PD3 + 2) % RS3) * 512;                                    \
+    constexpr uint32_t vn = ((K) % NV3) * VPL, vc = (((K) + 2) % NV3) * VPL;                  \
     cp_async_wait<PD3 - 1>();                                                                 \
     __syncthreads();                                                                          \
     fetch(it + PD3 + 2, sf);                                                                  \
+    Ap = lds16(cellA + sp1);                                                                  \
     if (form) {                                                                               \
-      const F4 Am = lds16(cellA + sm1), Ac = lds16(cellA + s0), Ap = lds16(cellA + sp1);      \
       const F4 up = ld_sh16(cellA - RB + s0), dn = ld_sh16(cellA + RB + s0);                  \
       const F4 Bq = lds16(cellB + s0);                                                        \
       const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
@@ -153,7 +157,6 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
         miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};                                      \
       }                                                                                       \
       const F4 wv = lap6(Am, Ac, Ap, up, dn, lft, rgt, miss);                                 \
-      F4 Vn;                                                                                  \
       Vn.a = fma2(CB, Bq.a, fma2(CA, Ac.a, mul2(CSx.a, wv.a)));                               \
       Vn.b = fma2(CB, Bq.b, fma2(CA, Ac.b, mul2(CSx.b, wv.b)));                               \
       if (EDGE) {                                                                             \
@@ -165,7 +168,6 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
       if (outw && io && it >= 1 && it <= last_it) f4_store(sp, Vn);                           \
       if (outw && it >= 2 && it <= last_it + 1) {                                             \
         const int r = q - 1;                                                                  \
-        const F4 Vm = lds16(cellV + vm), Vc = lds16(cellV + vc);                              \
         const F4 vu = ld_sh16(cellV + vc - 512), vd = ld_sh16(cellV + vc + 512);              \
         const float lv = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                              \
         const float rv = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                            \
@@ -194,8 +196,10 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
   acc[4] += (double)(q4.x + q4.y);        \
   q0 = q1 = q2 = q3 = q4 = f2(0.f);
   for (int it0 = 0; it0 < nit; it0 += RS3) {
-    NLSB_PLANE3(0) NLSB_PLANE3(1) NLSB_PLANE3(2) NLSB_FLUSH3
-    NLSB_PLANE3(3) NLSB_PLANE3(4) NLSB_PLANE3(5) NLSB_FLUSH3
+    NLSB_PLANE3(0, A0, A1, A2, V1, V2, V0) NLSB_PLANE3(1, A1, A2, A0, V2, V0, V1)
+    NLSB_PLANE3(2, A2, A0, A1, V0, V1, V2) NLSB_FLUSH3
+    NLSB_PLANE3(3, A0, A1, A2, V1, V2, V0) NLSB_PLANE3(4, A1, A2, A0, V2, V0, V1)
+    NLSB_PLANE3(5, A2, A0, A1, V0, V1, V2) NLSB_FLUSH3
   }
 #undef NLSB_FLUSH3
 #undef NLSB_PLANE3
