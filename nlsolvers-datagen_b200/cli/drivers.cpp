@@ -12,6 +12,11 @@
 //   NLS_KRYLOV_K=<k>          (default: the reference binary's k)
 //   NLS_SEED=<uint64>         (phi^4 noise key; default: wall clock, as stochastic_phi4.cuh:25)
 //   NLS_SEWI_VARIANT=reference|corrected
+//   NLS_NONLINEARITY=sine|dsine|sinh (KG / phi^4 executables) or cq|sat (NLSE):
+//                              the solvers the reference's build names without sources
+//                              (sine-Gordon, double / hyperbolic sine-Gordon, cubic-quintic,
+//                              saturable NLSE; forms in include/nlsb200.h); default: the
+//                              executable's own nonlinearity
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -144,6 +149,17 @@ int run(int argc, char **argv) {
   p.precision = NLS_FP64;
   if (const char *e = std::getenv("NLS_PRECISION")) p.precision = std::strcmp(e, "fp32") == 0 ? NLS_FP32 : NLS_FP64;
   if (const char *e = std::getenv("NLS_SEWI_VARIANT")) p.sewi_variant = std::strcmp(e, "corrected") == 0 ? 1 : 0;
+  if (const char *e = std::getenv("NLS_NONLINEARITY")) {
+    const char *names[] = {"poly", "sine", "dsine", "sinh", "cq", "sat"};
+    int kind = -1;
+    for (int i = 0; i < 6; ++i)
+      if (std::strcmp(e, names[i]) == 0) kind = i;
+    if (kind < 0) {
+      std::cerr << "NLS_NONLINEARITY must be one of poly, sine, dsine, sinh, cq, sat\n";
+      return 1;
+    }
+    p.nonlinearity = kind;
+  }
   const double *cd = reinterpret_cast<const double *>(c.data.data());
   const uint64_t n = u0.count();
   bool c_is_one = true;

@@ -103,3 +103,30 @@ def test_sp4_sv_2d_driver_seeded(tmp_path):
     traj = np.load(tmp_path / "traj.npy")
     otraj, _ = _oracle(spec, u0, v0, m, c)
     assert rel_l2(traj, otraj) < 1e-9
+
+
+@pytest.mark.parametrize("exe,kind", [("kg_gautschi_2d_dev", "sine"), ("nlse_2d_dev", "sat")])
+def test_driver_nonlinearity_env(tmp_path, exe, kind):
+    """NLS_NONLINEARITY turns an executable into one of the solvers the
+    reference's build names without sources (sine-Gordon on the Gautschi KG
+    executable, saturable NLSE on the SS2 one), in FP64 against the oracle."""
+    nl = _nl()
+    from nlsb200 import workloads as W
+    if exe.startswith("kg"):
+        spec, u0, v0, m, c = W.kg_case(32, 8.0, T=0.5, nt=50, ns=5, k=10, seed=31, precision=nl.FP64)
+        spec.nonlinearity = nl.NL_SINE
+        arrays = (("u0", u0), ("v0", v0), ("m", m), ("c", c))
+        args = [32, 32, 8.0, 8.0, tmp_path / "u0.npy", tmp_path / "v0.npy", tmp_path / "traj.npy",
+                tmp_path / "vel.npy", 0.5, 50, 5, tmp_path / "m.npy", tmp_path / "c.npy"]
+    else:
+        spec, u0, v0, m, c = W.nlse_case(32, 6.0, T=0.05, nt=50, ns=5, k=20, seed=32, precision=nl.FP64)
+        spec.nonlinearity = nl.NL_SAT
+        arrays = (("u0", u0), ("m", m), ("c", np.ones(u0.shape)))
+        args = [32, 32, 6.0, 6.0, tmp_path / "u0.npy", tmp_path / "traj.npy", 0.05, 50, 5, tmp_path / "m.npy",
+                tmp_path / "c.npy"]
+    for nm, a in arrays:
+        np.save(tmp_path / f"{nm}.npy", a)
+    _run(exe, args, {"NLS_NONLINEARITY": kind})
+    traj = np.load(tmp_path / "traj.npy")
+    otraj, _ = _oracle(spec, u0, v0, m, c)
+    assert rel_l2(traj, otraj) < 1e-9
