@@ -65,6 +65,8 @@ struct StepArgs {
   const int *lt_stride;  // device scalar: tiles per sequence section of the 2-D pass table
   const void *zeros;     // device buffer of zeros (source of out-of-grid rows)
   int scal_ready;        // 1: every pass published its scalars (f(T) reads them)
+  int v0_u;              // 1: V_0 of sequence 0 (the cosine start vector u) is not stored;
+                         //    the 2-D FP32 passes and the final pass read u_hi in its place
 };
 
 template <int DIM> struct Geo {

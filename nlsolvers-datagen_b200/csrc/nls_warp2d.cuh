@@ -835,7 +835,9 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
       const E *Vb = (const E *)a.V + (long long)(sq * kv) * a.vstride + S.addr(r);
 #pragma unroll
       for (int i = 0; i < NB; ++i)
-        vb[sq][i] = (io && i < kv - 1) ? ld16(Vb + (long long)i * a.vstride) : vzero<E>();
+        vb[sq][i] = (io && i < kv - 1)
+                        ? ld16((a.v0_u && sq == 0 && i == 0) ? (const E *)a.f.u_hi + S.addr(r) : Vb + (long long)i * a.vstride)
+                        : vzero<E>();
     }
     if constexpr (HC) cn2 = load_crow<E>(cf, S, r + 2);
     typename FR::Fld fld;
@@ -1665,11 +1667,14 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
   const bool hasB = j >= 2;
   const float *base = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
   const long long lane_off = s.off + S.col0;
-  const float *pA = (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
+  // V_0 of the cosine sequence is read from u_hi when the first pass did not store it
+  const bool u0A = a.v0_u && sq == 0 && j == 1, u0B = a.v0_u && sq == 0 && j == 2;
+  const float *pA = u0A ? (const float *)a.f.u_hi + lane_off : (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
   // LO at j = 1: the cosine sequence (0) streams u_lo as ring B (V_0 = u_hi there)
   const bool lo = LO && sq == 0;
-  const float *pB = lo ? (const float *)a.f.u_lo + lane_off
-                       : (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
+  const float *pB = lo    ? (const float *)a.f.u_lo + lane_off
+                    : u0B ? (const float *)a.f.u_hi + lane_off
+                          : (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
   float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
   F4 CSx, OPx, xmiss;
   {
@@ -1741,7 +1746,8 @@ __device__ __forceinline__ F4 f4_force(int kind, const F4 &u, const F4 &m, const
 template <bool EDGE, int SQ>
 __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM, float *pV, int P, int r0, int r1,
                                                 int ny, bool ld, bool io, const SlotDesc &s, const Strip &S,
-                                                int step, const F4 &OPx, const F4 &xmiss, double *acc) {
+                                                int step, const F4 &OPx, const F4 &xmiss, double *acc,
+                                                bool store = true) {
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
   const float2 P1 = f2(float(s.p1)), Q1 = f2(float(s.q1)), P3 = f2(float(s.p3)), Q3 = f2(float(s.q3));
   const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
@@ -1795,7 +1801,7 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
       F4 z = lap4(Xm, Xc, Xp, lft, rgt, miss);                                             \
       z.a = mul2(z.a, OPx.a);                                                              \
       z.b = mul2(z.b, OPx.b);                                                              \
-      if (io) f4_store(pV + c * P, Xc);                                                    \
+      if (io && store) f4_store(pV + c * P, Xc);                                           \
       q1 = fma2(z.a, Xc.a, fma2(z.b, Xc.b, q1));                                           \
       q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                             \
       q4 = fma2(Xc.a, Xc.a, fma2(Xc.b, Xc.b, q4));                                         \
@@ -1841,8 +1847,10 @@ static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const bool inner = r0 >= 2 && r1 <= ny - 2;
   if (sq == 0) {
-    if (inner) first_f32_march<false, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
-    else first_f32_march<true, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
+    // V_0 of the cosine sequence is u_hi itself: stored only when the passes read it from V
+    const bool st = !a.v0_u;
+    if (inner) first_f32_march<false, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st);
+    else first_f32_march<true, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st);
   } else {
     if (inner) first_f32_march<false, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
     else first_f32_march<true, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
