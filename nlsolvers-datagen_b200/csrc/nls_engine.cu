@@ -881,9 +881,11 @@ StepArgs base_args(const nls_pool *P, const TileSet &T, int group = 0) {
   a.zeros = P->zeros;
   a.scal_ready = 1;
   a.has_c = P->step_hc;
-  // the packed 2-D FP32 Gautschi forms read the cosine start vector from u_hi
-  a.v0_u = (P->dim == 2 && P->prec == NLS_FP32 && !P->cplx && !P->step_hc && !is_sv(P->method) &&
-            f32_first_packed() && f32_pass_form() == 3 && !use_tma())
+  // the packed FP32 Gautschi forms read the cosine start vector from u_hi
+  // (2-D and 3-D, c == 1)
+  const bool fam = P->prec == NLS_FP32 && !P->cplx && !P->step_hc && !is_sv(P->method);
+  a.v0_u = fam && ((P->dim == 2 && f32_first_packed() && f32_pass_form() == 3 && !use_tma()) ||
+                   (P->dim == 3 && use_k3()))
                ? 1
                : 0;
   return a;

@@ -248,8 +248,11 @@ static __global__ void __launch_bounds__(32 * W3, 1) k3_lanczos_f32(StepArgs a) 
   const long long vo = (long long)sq * a.kv;
   const float *base = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
   const long long row_off = s.off + (yin ? (long long)y * P : 0) + S.col0;
-  const float *rowA = (const float *)a.V + (vo + j - 1) * a.vstride + row_off;
-  const float *rowB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + row_off;
+  // V_0 of the cosine sequence is read from u_hi when the first pass did not store it
+  const bool u0A = a.v0_u && sq == 0 && j == 1, u0B = a.v0_u && sq == 0 && j == 2;
+  const float *rowA = u0A ? (const float *)a.f.u_hi + row_off : (const float *)a.V + (vo + j - 1) * a.vstride + row_off;
+  const float *rowB = u0B ? (const float *)a.f.u_hi + row_off
+                          : (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + row_off;
   float *rowJ = (float *)a.V + (vo + j) * a.vstride + row_off;
   const bool ldA = S.ld && yin, ldB = S.ld && yin && hasB;
   double acc[5] = {0, 0, 0, 0, 0};
@@ -369,7 +372,7 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
     const float2 zm = f2(float((q == 0) + (q == nz - 1)));
     const F4 miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};
     const F4 z = f4_mul(lap6(Xm, Xo, Xp, Xu, Xd, lft, rgt, miss), OPx);
-    if (S.io) f4_store(pV + (long long)q * PS, Xo);
+    if (S.io && (SQ == 1 || !a.v0_u)) f4_store(pV + (long long)q * PS, Xo);
     q1 = fma2(z.a, Xo.a, fma2(z.b, Xo.b, q1));
     q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));
     q4 = fma2(Xo.a, Xo.a, fma2(Xo.b, Xo.b, q4));
@@ -546,7 +549,7 @@ static __global__ void __launch_bounds__(32 * FH3, 1) k3_final_f32(StepArgs a) {
     F4 vb0[NB], vb1[NB];
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
-      vb0[i] = ldrow(Vb0 + o + (long long)i * a.vstride, io && i < kv - 1);
+      vb0[i] = ldrow((a.v0_u && i == 0 ? pH : Vb0 + (long long)i * a.vstride) + o, io && i < kv - 1);
       vb1[i] = ldrow(Vb1 + o + (long long)i * a.vstride, io && i < kv - 1);
     }
     const F4 fh = ldrow(pH + o, io), fl = ldrow(pL + o, io), fd = ldrow(pD + o, io);
