@@ -354,19 +354,34 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
   float *pV = (float *)a.V + (long long)(SQ * a.kv) * a.vstride + row_off;
   const bool hu = y > 0, hd = y < ny - 1;
   const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
-  auto xrow = [&](int q, long long dy) -> F4 {  // x at (y + dy, q)
-    const bool ok = S.ld && q >= 0 && q < nz;
-    const long long o = (long long)q * PS + dy * P;
-    const F4 u = ldrow(pU + o, ok);
-    const F4 m = SQ == 1 ? ldrow(pM + o, ok) : F4{f2(0.f), f2(0.f)};
-    return src3<SQ>(u, m, s, step, S.col0, nx, ((long long)q * ny + y + dy) * nx, noisy, ok);
+  // raw rows (u, and m for the sinc sequence) are loaded one plane ahead of
+  // the plane whose stencil needs them, so a plane's loads overlap the
+  // previous plane's arithmetic
+  struct Raw {
+    F4 u, m;
+    int q;
+    long long dy;
   };
-  F4 Xm = xrow(p0 - 1, 0), Xo = xrow(p0, 0);
+  auto load = [&](int q, long long dy) -> Raw {
+    const bool ok = S.ld && q >= 0 && q < nz && (dy == 0 || (dy < 0 ? hu : hd));
+    const long long o = (long long)q * PS + dy * P;
+    Raw r{ldrow(pU + o, ok), SQ == 1 ? ldrow(pM + o, ok) : F4{f2(0.f), f2(0.f)}, q, dy};
+    return r;
+  };
+  auto make = [&](const Raw &r) -> F4 {
+    const bool ok = S.ld && r.q >= 0 && r.q < nz && (r.dy == 0 || (r.dy < 0 ? hu : hd));
+    return src3<SQ>(r.u, r.m, s, step, S.col0, nx, ((long long)r.q * ny + y + r.dy) * nx, noisy, ok);
+  };
+  F4 Xm = make(load(p0 - 1, 0)), Xo = make(load(p0, 0));
+  Raw Rp = load(p0 + 1, 0), Ru = load(p0, -1), Rd = load(p0, 1);
   float2 q1 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
   for (int q = p0; q < p1; ++q) {
-    const F4 Xp = xrow(q + 1, 0);
-    const F4 Xu = hu ? xrow(q, -1) : F4{f2(0.f), f2(0.f)};
-    const F4 Xd = hd ? xrow(q, 1) : F4{f2(0.f), f2(0.f)};
+    const F4 Xp = make(Rp), Xu = make(Ru), Xd = make(Rd);
+    if (q + 1 < p1) {
+      Rp = load(q + 2, 0);
+      Ru = load(q + 1, -1);
+      Rd = load(q + 1, 1);
+    }
     const float lft = __shfl_up_sync(0xffffffffu, Xo.b.y, 1);
     const float rgt = __shfl_down_sync(0xffffffffu, Xo.a.x, 1);
     const float2 zm = f2(float((q == 0) + (q == nz - 1)));
