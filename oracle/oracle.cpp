@@ -1,8 +1,10 @@
 // FP64 CPU oracle: restatement of the reference's arithmetic for the Lanczos
 // exponential integrators. TEST INFRASTRUCTURE ONLY (see oracle.h): only the
 // tests, the smoke check and the CPU-baseline legs of bench.py may call it.
-// PARITY UNPINNED: the reference has no tests or golden vectors and no CPU
-// path; citations below name the reference lines each function restates.
+// The reference has no tests or golden vectors and no CPU path; citations
+// below name the reference lines each function restates. Pinned for the KG
+// integrators against the reference's own compiled device code (oracle.h);
+// unpinned for the NLSE integrators and the phi^4 noise.
 #include "oracle.h"
 
 #include <algorithm>

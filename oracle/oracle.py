@@ -4,10 +4,14 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
 the CPU-baseline legs of ``bench.py`` as the checker / timed CPU baseline. The
 product (``nlsolvers-datagen_b200``) never imports it.
 
-PARITY UNPINNED: the reference (konradha/nlsolvers-datagen) has no tests,
-golden vectors or CPU path and cannot be built here; the oracle restates the
-arithmetic of device/include/*.hpp line by line (see oracle.cpp) and is
-cross-checked against dense numpy/scipy answers in tests/test_oracle_kat.py.
+The reference (konradha/nlsolvers-datagen) has no tests, golden vectors or
+CPU path; the oracle restates the arithmetic of device/include/*.hpp line by
+line (see oracle.cpp) and is cross-checked against dense numpy/scipy answers in
+tests/test_oracle_kat.py. PINNED for the KG Gautschi and Stormer-Verlet
+integrators against the reference's own device code, compiled by
+oracle/Makefile into oracle/_ref (tests/test_gpu_reference_pin.py); UNPINNED
+for the NLSE integrators (that code needs Eigen) and the phi^4 noise (seeded
+from the wall clock).
 """
 from __future__ import annotations
 

@@ -1,0 +1,94 @@
+// Runs the reference's own device code for the KG integrators, compiled from
+// its sources (device/include/kg_single.cuh: step, step_sv; matfunc_real.hpp,
+// lanczos.hpp, spmv.hpp: the Lanczos matrix functions; boundaries.cuh:
+// neumann_bc_no_velocity_blocking and its 3-D form). Test infrastructure: the
+// tests compare the oracle and the engine with it.
+//
+// The orchestration is restated here because the reference's own files for it
+// need Eigen, which this image lacks: the state set-up of kg_dev.hpp:32-80
+// (u_past = u0 - dt v0, snapshot 0 = (u0, v0)), the boundary choice of
+// kg_dev.hpp:116-121, the device-side snapshot store of kg_dev.hpp:123-131
+// (transferred once at the end, kg_dev.hpp:107-114) and the driver loop of
+// kg_driver_dev_2d.cpp:144-153 (step, boundary copy, snapshot every nt/ns
+// steps). If loop_ms is not null it receives the duration of that loop (CUDA
+// events on the default stream, which all of the reference's work uses). The caller passes the operator as
+// CSR arrays (A = -L for Gautschi, L for Stormer-Verlet,
+// kg_driver_dev_2d.cpp:105-108, kg_sv_driver_dev_2d.cpp:102-105), since the
+// reference assembles it with Eigen (laplacians.hpp). Square and cubic grids
+// only, as KGESolverDevice (kg_dev.hpp:38-45).
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "boundaries.cuh"
+#include "kg_single.cuh"
+
+extern "C" int ref_kg_run(int32_t dim, int32_t method, int32_t nx, const int32_t *row_ptr, const int32_t *col_ind,
+                          const double *vals, int32_t nnz, int32_t k, const double *u0, const double *v0,
+                          const double *m, double dt, int32_t nt, int32_t ns, double *traj, double *vel,
+                          double *loop_ms) {
+  if ((dim != 2 && dim != 3) || nx < 3 || k < 2 || nt < 1 || ns < 1 || nt < ns) return -3;
+  const uint32_t n = (uint32_t)nx * (uint32_t)nx * (dim == 3 ? (uint32_t)nx : 1u);
+  if (row_ptr[0] != 0 || row_ptr[n] != nnz) return -3;
+  int *d_row = nullptr, *d_col = nullptr;
+  double *d_val = nullptr, *d_u = nullptr, *d_v = nullptr, *d_up = nullptr, *d_b1 = nullptr, *d_b2 = nullptr,
+         *d_b3 = nullptr, *d_m = nullptr, *d_traj = nullptr, *d_vel = nullptr;
+  cudaMalloc(&d_row, (n + 1) * sizeof(int));
+  cudaMalloc(&d_col, (size_t)nnz * sizeof(int));
+  cudaMalloc(&d_val, (size_t)nnz * sizeof(double));
+  for (double **p : {&d_u, &d_v, &d_up, &d_b1, &d_b2, &d_b3, &d_m}) cudaMalloc(p, n * sizeof(double));
+  cudaMalloc(&d_traj, (size_t)ns * n * sizeof(double));
+  cudaMalloc(&d_vel, (size_t)ns * n * sizeof(double));
+  cudaMemcpy(d_row, row_ptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_col, col_ind, (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_val, vals, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice);
+  std::vector<double> up(n);
+  for (uint32_t i = 0; i < n; ++i) up[i] = u0[i] - dt * v0[i];
+  cudaMemcpy(d_u, u0, n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_v, v0, n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_up, up.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_m, m, n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_traj, u0, n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(d_vel, v0, n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaEvent_t ev[2];
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
+  int rc = 0;
+  try {
+    MatrixFunctionApplicatorReal matfunc(d_row, d_col, d_val, n, (uint32_t)k, (uint32_t)nnz);
+    const dim3 block(256), grid((n + 255) / 256);
+    const int freq = nt / ns;
+    const uint32_t e = (uint32_t)nx;
+    cudaDeviceSynchronize();
+    cudaEventRecord(ev[0], 0);
+    for (int i = 1; i < nt; ++i) {
+      if (method == 0)
+        device::KGESolver::step(d_v, d_u, d_up, d_b1, d_b2, d_b3, &matfunc, d_m, dt, n, grid, block);
+      else
+        device::KGESolver::step_sv(d_v, d_u, d_up, d_b1, d_b2, d_b3, &matfunc, d_m, dt, n, grid, block);
+      if (dim == 2)
+        neumann_bc_no_velocity_blocking<double>(d_u, e, e);
+      else
+        neumann_bc_no_velocity_blocking_3d<double>(d_u, e, e, e);
+      if (i % freq == 0 && i / freq < ns) {
+        cudaMemcpy(d_traj + (size_t)(i / freq) * n, d_u, n * sizeof(double), cudaMemcpyDeviceToDevice);
+        cudaMemcpy(d_vel + (size_t)(i / freq) * n, d_v, n * sizeof(double), cudaMemcpyDeviceToDevice);
+      }
+    }
+    cudaEventRecord(ev[1], 0);
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = -1;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    if (loop_ms) *loop_ms = ms;
+    cudaMemcpy(traj, d_traj, (size_t)ns * n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(vel, d_vel, (size_t)ns * n * sizeof(double), cudaMemcpyDeviceToHost);
+  } catch (...) {  // the reference's error checks throw (pragmas.hpp)
+    rc = -2;
+  }
+  for (void *p : {(void *)d_row, (void *)d_col, (void *)d_val, (void *)d_u, (void *)d_v, (void *)d_up, (void *)d_b1,
+                  (void *)d_b2, (void *)d_b3, (void *)d_m, (void *)d_traj, (void *)d_vel})
+    cudaFree(p);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  return rc;
+}
