@@ -307,7 +307,8 @@ def run_small(args, lrank):
     else:
         cases = make_batch(B, 0, k)
         cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
-    pool = Pool(method, dim, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg)
+    pool = Pool(method, dim, k, FP32, capacity_points=cap, max_slots=B, segment=args.seg,
+                final_segment=args.fseg if dim == 2 else None)
     for cs in cases:
         assert pool.admit(*cs) is not None
     pool.step(args.warmup)
@@ -315,6 +316,7 @@ def run_small(args, lrank):
     pool.sync()
     pass_ms, _ = pool.time_pass(2, 20)
     print(json.dumps({"small": True, "method": int(method), "dim": dim, "n": cases[0][0].nx, "batch": B, "k": k, "seg": args.seg,
+                      "fseg": args.fseg,
                       "ms_per_step": ms / args.steps,
                       "pass_ms": pass_ms, "kernels_per_step": pool.kernels_per_step()}), flush=True)
     pool.close()
@@ -344,14 +346,18 @@ def run_ours(args, ws, rank, lrank):
     n = cases[0][0].n
     cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
 
+    # the final pass sums nothing across tiles and keeps its own 16-row tiles
+    # (more warps than the passes' segments give it)
     def make_pool(seg):
-        return Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=seg)
+        return Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=seg, final_segment=16)
 
     def admit_all(pool):
         for cs in cases:
             assert pool.admit(*cs) is not None
 
-    seg, seg_times = autotune.choose_segment(make_pool, admit_all, candidates=(16, 32, 64), steps=3)
+    # 25 rows: 12 segments x 3 strips x 2 sequences x 32 trajectories per group
+    # = 2304 warps, one wave of 16 warps on each of the 148 SMs
+    seg, seg_times = autotune.choose_segment(make_pool, admit_all, candidates=(16, 25, 28, 32), steps=6)
     seg = bcast_int(seg, ws)  # every rank runs rank 0's tiling
     pool = make_pool(seg)
     admit_all(pool)
@@ -394,7 +400,7 @@ def run_ours(args, ws, rank, lrank):
         tr = nl.pinned_empty((spec.ns,) + spec.shape)
         ve = nl.pinned_empty((spec.ns,) + spec.shape)
         pinned.append((spec, pu, pv, pm, c, tr, ve))
-    epool = Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=seg)
+    epool = make_pool(seg)
     barrier(ws)
     t0 = time.perf_counter()
     slots = [epool.admit(spec, pu, pv, pm, c, traj=tr, vel=ve)
@@ -420,7 +426,7 @@ def run_ours(args, ws, rank, lrank):
         "data": "synthetic (seeded kink/Gaussian u0, m = 1 + 0.2 GRF(k^-3))",
         "config": {"workload": "KG 2-D Gautschi batch, 64 x 300^2 on [-15,15]^2, dt=0.005, nt=6000, ns=50",
                    "global_batch": B * ws, "per_gpu_batch": B, "grid": [CFG["n"], CFG["n"]],
-                   "k": k, "k_autotune_err": kreport, "segment_rows": seg,
+                   "k": k, "k_autotune_err": kreport, "segment_rows": seg, "final_segment_rows": 16,
                    "segment_ms": seg_times, "parallelism": f"trajectory shards x{ws}",
                    "l2": "working set 0.6 GB per GPU >> 126 MB L2 (no flush needed)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -458,6 +464,7 @@ def main():
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
     ap.add_argument("--seg", type=int, default=32, help="segment rows (planes in 3-D) of the --small case")
+    ap.add_argument("--fseg", type=int, default=0, help="2-D final-pass segment rows of the --small case (0: --seg)")
     ap.add_argument("--nlse", action="store_true", help="--small case as NLSE 2-D SS2 boxes of 200^2 (k = 12)")
     ap.add_argument("--dim3", type=int, default=0,
                     help="--small case as KG 3-D boxes of DIM3^3 points (0: the 2-D 300^2 workload)")

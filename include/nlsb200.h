@@ -192,6 +192,10 @@ int nls_pool_usage(nls_pool *pool, int32_t *occupied, int64_t *free_points);
 int nls_pool_set_graphs(nls_pool *pool, int32_t enable);
 /* Rows of the march segment (tile length along y in 2-D / z in 3-D). */
 int nls_pool_set_segment(nls_pool *pool, int32_t rows);
+/* 2-D pools: rows of the final pass's tiles, which may differ from the
+   segment of the Lanczos passes (0: the same). The final pass sums nothing
+   across tiles, so results do not depend on it. */
+int nls_pool_set_final_segment(nls_pool *pool, int32_t rows);
 /* Time `iters` launches of Lanczos pass j (1 <= j <= k-2) on the current state
    (over every slot group of the step, launched side by side as the step does)
    with CUDA events; *ms = mean duration of one launch; *points = grid points

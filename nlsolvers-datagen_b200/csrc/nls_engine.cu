@@ -530,6 +530,12 @@ struct TileSet {
   int *d_ntt1 = nullptr, *d_ntt2 = nullptr;
   int tcap = 0, tt_live = 0, tt_count2 = 0;
   std::vector<TileDesc> tt;
+  // 2-D final pass: warp tiles of its own segment length (it sums nothing
+  // across tiles, so its tiling does not change any result)
+  TileDesc *d_ft = nullptr;
+  int *d_nft = nullptr;
+  int fcap = 0, ft_live = 0;
+  std::vector<TileDesc> ft;
 };
 
 }  // namespace
@@ -571,6 +577,7 @@ struct nls_pool {
   // 16 x 220^3 measured 16.37 / 15.81 / 15.33 / 15.28 / 15.14 / 15.20 ms per
   // step at 32 / 40 / 58 / 70 / 88 / 110 planes
   int seg2 = 32, seg3 = 88;  // march lengths (rows in 2-D, planes in 3-D)
+  int segf2 = 0;             // rows of the 2-D final pass's tiles (0: seg2)
   cudaStream_t stream = nullptr, copy_stream = nullptr, stream2 = nullptr;
   cudaEvent_t ev_step = nullptr, ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = true;
@@ -579,6 +586,7 @@ struct nls_pool {
   void *graph_part = nullptr;
   int graph_lcap = -1, graph_tcap = -1;
   int graph_split = -1, graph_tiles2 = -1, graph_lcap2 = -1, graph_tcap2 = -1;
+  int graph_fcap = -1, graph_fcap2 = -1;
   int step_hc = 0;  // some stepped slot carries a c field
   int ring_blocks = 1;
   int kernels_per_step = 0;
@@ -634,7 +642,8 @@ void pool_free_device(nls_pool *P) {
                   P->main.d_ntt1, P->main.d_ntt2, P->first.d_tt, P->first.d_ntt1,
                   P->first.d_ntt2, P->main2.d_tiles, P->main2.d_ntiles, P->main2.d_list,
                   P->main2.d_nlist, P->main2.d_lt, P->main2.d_nlt1, P->main2.d_nlt2, P->main2.d_tt,
-                  P->main2.d_ntt1, P->main2.d_ntt2, P->zeros, P->d_diag_part, P->d_diag_out, P->d_diag_ticket};
+                  P->main2.d_ntt1, P->main2.d_ntt2, P->zeros, P->d_diag_part, P->d_diag_out, P->d_diag_ticket,
+                  P->main.d_ft, P->main.d_nft, P->main2.d_ft, P->main2.d_nft, P->first.d_ft, P->first.d_nft};
   for (void *b : bufs)
     if (b) cudaFree(b);
 }
@@ -648,22 +657,23 @@ int64_t slot_padded(const nls_problem &p, int32_t &pitch) {
 // Tiles of one slot. 2-D: warp strips of W <= 30 output vectors (16 bytes each)
 // x seg rows; 3-D: 32x8 columns x seg planes. The tiling depends only on the
 // slot, so its reduction order is the same alone and in any batch.
-void slot_tiles(const nls_pool *P, int slot, const SlotDesc &s, std::vector<TileDesc> &out) {
+void slot_tiles(const nls_pool *P, int slot, const SlotDesc &s, std::vector<TileDesc> &out, int seg2 = 0) {
   int local = 0;
   if (P->dim == 2) {
+    const int seg = seg2 > 0 ? seg2 : P->seg2;
     const int N = (int)(16 / P->esz);
     const int wmax = N == 1 ? HaloLanes<1>::WMAX : HaloLanes<2>::WMAX;
     const int nvec = (s.nx + N - 1) / N;
     const int nseg = (nvec + wmax - 1) / wmax;
     const int W = (nvec + nseg - 1) / nseg;
-    for (int p0 = 0; p0 < s.ny; p0 += P->seg2)
+    for (int p0 = 0; p0 < s.ny; p0 += seg)
       for (int g = 0; g < nseg; ++g) {
         TileDesc t;
         t.slot = slot;
         t.x0 = g * W * N;
         t.y0 = std::min(W, nvec - g * W);
         t.p0 = p0;
-        t.p1 = std::min(s.ny, p0 + P->seg2);
+        t.p1 = std::min(s.ny, p0 + seg);
         t.local = local++;
         out.push_back(t);
       }
@@ -833,6 +843,20 @@ int rebuild_tables(nls_pool *P) {
       CK(cudaMemcpyAsync(T->d_ntt1, &T->tt_live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
       CK(cudaMemcpyAsync(T->d_ntt2, &T->tt_count2, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     }
+    if (P->dim == 2) {
+      T->ft.clear();
+      for (int sidx : T->list) slot_tiles(P, sidx, P->sd[sidx], T->ft, P->segf2);
+      T->ft_live = (int)T->ft.size();
+      if (T->ft_live > T->fcap || !T->d_ft) {
+        if (T->d_ft) cudaFree(T->d_ft);
+        T->d_ft = nullptr;
+        T->fcap = (std::max(T->ft_live, 64) + 63) / 64 * 64;
+        CK(cudaMalloc(&T->d_ft, sizeof(TileDesc) * T->fcap));
+      }
+      if (T->ft_live)
+        CK(cudaMemcpyAsync(T->d_ft, T->ft.data(), sizeof(TileDesc) * T->ft_live, cudaMemcpyHostToDevice, P->stream));
+      CK(cudaMemcpyAsync(T->d_nft, &T->ft_live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
+    }
     if (T->live) CK(cudaMemcpyAsync(T->d_tiles, T->tiles.data(), sizeof(TileDesc) * T->live, cudaMemcpyHostToDevice, P->stream));
     CK(cudaMemcpyAsync(T->d_ntiles, &T->live, sizeof(int), cudaMemcpyHostToDevice, P->stream));
     if (T->nlist) CK(cudaMemcpyAsync(T->d_list, T->list.data(), sizeof(int) * T->nlist, cudaMemcpyHostToDevice, P->stream));
@@ -956,6 +980,11 @@ int run_krylov(nls_pool *P, const TileSet &T, const Launch &L, StepArgs a, int &
     f.ntiles = T.d_ntt1;
     f.lt_stride = T.d_ntt1;
     CK(L.final_[hc](f, T.tcap, st));
+  } else if (P->dim == 2) {
+    StepArgs f = a;
+    f.tiles = T.d_ft;
+    f.ntiles = T.d_nft;
+    CK(L.final_[hc](f, T.fcap, st));
   } else {
     CK(L.final_[hc](a, grid, st));
   }
@@ -1046,8 +1075,9 @@ int run_main_step(nls_pool *P) {
   if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks ||
       P->graph_hc != P->step_hc || P->graph_part != (void *)P->part ||
       P->graph_lcap != P->main.lcap || P->graph_tcap != P->main.tcap || P->graph_split != sp ||
+      P->graph_fcap != P->main.fcap ||
       (sp && (P->graph_tiles2 != P->main2.cap || P->graph_lcap2 != P->main2.lcap ||
-              P->graph_tcap2 != P->main2.tcap))) {
+              P->graph_tcap2 != P->main2.tcap || P->graph_fcap2 != P->main2.fcap))) {
     if (P->gexec) {
       cudaGraphExecDestroy(P->gexec);
       P->gexec = nullptr;
@@ -1074,6 +1104,8 @@ int run_main_step(nls_pool *P) {
     P->graph_tiles2 = P->main2.cap;
     P->graph_lcap2 = P->main2.lcap;
     P->graph_tcap2 = P->main2.tcap;
+    P->graph_fcap = P->main.fcap;
+    P->graph_fcap2 = P->main2.fcap;
   }
   CK(cudaGraphLaunch(P->gexec, P->stream));
   return NLS_OK;
@@ -1429,6 +1461,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
     if (!rc) rc = al((void **)&T->d_nlt1, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlt2, sizeof(int));
     if (!rc) rc = al((void **)&T->d_ntiles, sizeof(int));
+    if (!rc) rc = al((void **)&T->d_nft, sizeof(int));
     if (!rc) rc = al((void **)&T->d_nlist, sizeof(int));
     if (!rc) rc = al((void **)&T->d_list, sizeof(int) * max_slots);
   }
@@ -1801,6 +1834,14 @@ int nls_pool_set_segment(nls_pool *P, int32_t rows) {
     P->seg2 = rows;
   else
     P->seg3 = rows;
+  P->tables_dirty = true;
+  return NLS_OK;
+}
+
+int nls_pool_set_final_segment(nls_pool *P, int32_t rows) {
+  if (!P || rows < 0) return fail(NLS_ERR_INVALID_ARG, "bad segment");
+  if (P->dim != 2) return fail(NLS_ERR_INVALID_ARG, "the final-pass segment applies to 2-D pools");
+  P->segf2 = rows;
   P->tables_dirty = true;
   return NLS_OK;
 }

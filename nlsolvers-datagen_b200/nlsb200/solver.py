@@ -239,7 +239,7 @@ class Pool:
 
     def __init__(self, method: int, dim: int, k: int | None, precision: int,
                  capacity_points: int, max_slots: int, graphs: bool = True,
-                 segment: int | None = None):
+                 segment: int | None = None, final_segment: int | None = None):
         if k is None:
             p = _lib.Problem()
             check(lib().nls_problem_defaults(ctypes.byref(p), method, dim))
@@ -253,6 +253,8 @@ class Pool:
             check(lib().nls_pool_set_graphs(self._p, 0))
         if segment:
             check(lib().nls_pool_set_segment(self._p, int(segment)))
+        if final_segment:
+            check(lib().nls_pool_set_final_segment(self._p, int(final_segment)))
 
     def admit(self, spec: Spec, u0, v0, m, c=None, traj=None, vel=None, out_npy=None):
         """Returns the slot id, or None when the pool is full right now.
