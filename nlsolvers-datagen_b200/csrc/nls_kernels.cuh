@@ -743,6 +743,183 @@ __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
   }
 }
 
+// Low-latency f(T~)e_1 for the real symmetric tridiagonal T~ = tridiag(e, d, e)
+// (k <= KP; d, e in every lane's registers; lane i returns c_i). f is applied
+// to the eigenvalues as the reference does (matfunc_real.hpp:212-238,
+// matfunc_complex.hpp:281-300): the square-root kinds of |lambda|, EXP and
+// SINC of lambda. Let g be the entire function that equals f on lambda >= 0
+// (cos(t sqrt(l)) = sum (-t^2 l)^n / (2n)!, sinc^2(t sqrt(l)) =
+// sum (-4 t^2 l)^n 2 / (2n+2)!; EXP and SINC are entire already). Then
+//   f(T~)e_1 = g(T~)e_1 + sum over lambda_i < 0 of (f - g)(lambda_i) z_i[0] z_i.
+// g(T~)e_1 is a Taylor series of lane-parallel tridiagonal products, summed
+// until the term bound |a_n| rho^n (rho: Gershgorin radius) is below 1e-18; it
+// is used while the argument bound (t^2 rho for the square-root kinds, |tau|
+// rho otherwise) is at most 4. The truncated Lanczos matrix (last diagonal 0)
+// has one negative eigenvalue when its leading block is positive definite
+// (Schur complement -b^2 e^T T_{k-1}^-1 e < 0; interlacing keeps the others
+// >= 0): lambda_1 is found by Laguerre's method from the left of the spectrum
+// on the characteristic polynomial (monotone and cubically convergent for a
+// polynomial with real roots), a Sturm count at -1e-12 rho checks that it is
+// the only eigenvalue below -1e-12 rho, and its eigenvector is
+// u_i = (-1)^i p_i(lambda_1) / (e_0 ... e_{i-1}) with p_i the leading minors,
+// so z_1[0] z_1 = u / |u|^2. Any other case (a larger argument, several
+// negative eigenvalues, a zero subdiagonal entry, no convergence, non-finite
+// values) returns false and the caller runs the QL path. Agreement with a
+// dense eigendecomposition is about 1e-15.
+template <int KP>
+__device__ bool ftri_fast(int k, const double *d, const double *e, int lane, int fk, double tr, double ti,
+                          double &cr, double &ci) {
+  // lane-distributed rows of T~ (lanes >= k hold zeros)
+  double my_d = 0.0, my_el = 0.0, my_eh = 0.0;
+#pragma unroll
+  for (int q = 0; q < KP; ++q) {
+    if (q == lane) {
+      my_d = d[q];
+      my_eh = e[q];
+    }
+    if (q + 1 == lane) my_el = e[q];
+  }
+  double rho = lane < k ? fabs(my_d) + my_el + my_eh : 0.0;
+  double lo = lane < k ? my_d - my_el - my_eh : 1e300;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+  }
+  const bool sqk = fk == FK_COS_SQRT || fk == FK_SINC2_SQRT;
+  const double arg = sqk ? tr * tr * rho : (fk == FK_EXP ? sqrt(tr * tr + ti * ti) : fabs(tr)) * rho;
+  if (!(arg <= 4.0) || !isfinite(rho)) return false;
+  // Taylor series of g(T~)e_1: c = sum a_n x_n, x_n = T~^n e_1 (T~^2n for SINC)
+  double x = lane == 0 ? 1.0 : 0.0;
+  double ar = 1.0, ai = 0.0;  // a_0 = 1 for every kind
+  cr = x;
+  ci = 0.0;
+  double rpow = 1.0;
+  for (int n = 1; n <= 80; ++n) {
+    const int reps = fk == FK_SINC ? 2 : 1;
+    for (int r = 0; r < reps; ++r) {
+      const double xu = __shfl_up_sync(0xffffffffu, x, 1), xd = __shfl_down_sync(0xffffffffu, x, 1);
+      x = fma(my_d, x, fma(my_el, xu, my_eh * xd));
+      rpow *= rho;
+    }
+    if (fk == FK_COS_SQRT) {
+      ar *= -(tr * tr) / ((2.0 * n - 1.0) * (2.0 * n));
+    } else if (fk == FK_SINC2_SQRT) {
+      ar *= -4.0 * (tr * tr) / ((2.0 * n + 1.0) * (2.0 * n + 2.0));
+    } else if (fk == FK_EXP) {
+      const double nr = (ar * tr - ai * ti) / n, ni = (ar * ti + ai * tr) / n;
+      ar = nr;
+      ai = ni;
+    } else {
+      ar *= -(tr * tr) / ((2.0 * n) * (2.0 * n + 1.0));
+    }
+    cr = fma(ar, x, cr);
+    ci = fma(ai, x, ci);
+    if ((fabs(ar) + fabs(ai)) * rpow < 1e-18) break;
+    if (n == 80) return false;
+  }
+  if (!sqk) return true;
+  // the negative eigenvalue of the truncated matrix: Laguerre from the left
+  auto minors = [&](double xv, double &p, double &dp, double &d2p) {
+    double p0 = 1.0, p1 = d[0] - xv, q0 = 0.0, q1 = -1.0, r0 = 0.0, r1 = 0.0;
+#pragma unroll
+    for (int i = 1; i < KP; ++i) {
+      if (i < k) {
+        const double e2 = e[i - 1] * e[i - 1], di = d[i] - xv;
+        const double p2 = di * p1 - e2 * p0, q2 = di * q1 - e2 * q0 - p1, r2 = di * r1 - e2 * r0 - 2.0 * q1;
+        p0 = p1;
+        p1 = p2;
+        q0 = q1;
+        q1 = q2;
+        r0 = r1;
+        r1 = r2;
+      }
+    }
+    p = p1;
+    dp = q1;
+    d2p = r1;
+  };
+  const double kd = (double)k;
+  double xv = lo - 1e-3 * rho - 1e-300;
+  bool conv = false;
+  for (int it = 0; it < 32; ++it) {
+    double p, dp, d2p;
+    minors(xv, p, dp, d2p);
+    if (!(isfinite(p) && isfinite(dp) && isfinite(d2p))) return false;
+    if (p <= 0.0) {  // p > 0 left of the smallest eigenvalue: at it within rounding
+      conv = true;
+      break;
+    }
+    const double G = dp / p, H = G * G - d2p / p;
+    const double disc = fmax((kd - 1.0) * (kd * H - G * G), 0.0);
+    const double dx = -kd / (G - sqrt(disc));
+    if (!isfinite(dx)) return false;
+    if (dx <= 0.0) {
+      conv = true;
+      break;
+    }
+    xv += dx;
+    if (dx <= 2e-16 * fabs(xv) + 1e-300) {
+      conv = true;
+      break;
+    }
+  }
+  if (!conv) return false;
+  const double lam1 = xv, dl = 1e-12 * rho;
+  if (lam1 >= -dl) return true;  // no eigenvalue below -1e-12 rho: f = g on the spectrum to that bound
+  // Sturm count at -dl: sign changes of p_0 .. p_k must be exactly one
+  {
+    double p0 = 1.0, p1 = d[0] + dl;
+    int nu = (p1 < 0.0) ? 1 : 0;
+    bool zero = p1 == 0.0;
+#pragma unroll
+    for (int i = 1; i < KP; ++i) {
+      if (i < k) {
+        const double p2 = (d[i] + dl) * p1 - e[i - 1] * e[i - 1] * p0;
+        nu += ((p2 < 0.0) != (p1 < 0.0)) ? 1 : 0;
+        zero = zero || p2 == 0.0;
+        p0 = p1;
+        p1 = p2;
+      }
+    }
+    if (zero || nu != 1) return false;
+  }
+  // eigenvector of lambda_1 from the leading minors at lambda_1 (u_0 = 1)
+  double u = 0.0;
+  {
+    double p0 = 1.0, p1 = d[0] - lam1, E = 1.0, sg = 1.0;
+    bool ok = true;
+    if (lane == 0) u = 1.0;
+#pragma unroll
+    for (int i = 1; i < KP; ++i) {
+      if (i < k) {
+        E *= e[i - 1];
+        sg = -sg;
+        ok = ok && e[i - 1] > 1e-150;
+        if (i == lane) u = sg * p1 / E;
+        const double p2 = (d[i] - lam1) * p1 - e[i - 1] * e[i - 1] * p0;
+        p0 = p1;
+        p1 = p2;
+      }
+    }
+    if (!ok) return false;
+  }
+  double uu = u * u;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) uu += __shfl_xor_sync(0xffffffffu, uu, o);
+  if (!(uu > 0.0) || !isfinite(uu)) return false;
+  const double xa = tr * sqrt(-lam1);
+  double corr;
+  if (fk == FK_COS_SQRT) {
+    corr = cos(xa) - cosh(xa);
+  } else {
+    const double sa = sin(xa) / xa, sh = sinh(xa) / xa;
+    corr = sa * sa - sh * sh;
+  }
+  cr = fma(corr, u / uu, cr);
+  return true;
+}
+
 // Register-resident f(T) for k <= KP (KP = 8, 12, 16): the same T assembly,
 // implicit QL sweeps and coefficients as k_ftri, but every lane of the warp
 // runs the scalar QL recurrences itself on register copies of d and e (the
@@ -812,10 +989,14 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
       }
     }
   }
+  const int fk = a.fkind[sq];
+  const double ftr = a.tsc[sq][0] * s.dt, fti = a.tsc[sq][1] * s.dt;
+  double cr = 0.0, ci = 0.0;
+  int status = 0;
+  if (!ftri_fast<KP>(k, d, e, lane, fk, ftr, fti, cr, ci)) {
   double Z[KP];
 #pragma unroll
   for (int i = 0; i < KP; ++i) Z[i] = i == lane ? 1.0 : 0.0;
-  int status = 0;
 #pragma unroll
   for (int l = 0; l < KP; ++l) {
     if (l >= k || status) break;
@@ -888,8 +1069,7 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
       }
     }
   }
-  // f(lambda_i) Z[0][i] for i = lane, then c_r = delta_r sum_i Z[r][i] f_i Z[0][i]
-  const int fk = a.fkind[sq];
+  // f(lambda_i) Z[0][i] for i = lane, then c_r = sum_i Z[r][i] f_i Z[0][i]
   double lam = 0.0, z0 = 0.0;
 #pragma unroll
   for (int i = 0; i < KP; ++i) {
@@ -901,11 +1081,10 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
   }
   double fr = 0.0, fi = 0.0;
   if (lane < k) {
-    fval(fk, lam, a.tsc[sq][0] * s.dt, a.tsc[sq][1] * s.dt, fr, fi);
+    fval(fk, lam, ftr, fti, fr, fi);
     fr *= z0;
     fi *= z0;
   }
-  double cr = 0.0, ci = 0.0;
 #pragma unroll
   for (int i = 0; i < KP; ++i) {
     const double gr = __shfl_sync(0xffffffffu, fr, i), gi = __shfl_sync(0xffffffffu, fi, i);
@@ -914,6 +1093,8 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
       ci += gi * Z[i];
     }
   }
+  }  // QL path
+  // c_r = delta_r (f(T~)e_1)_r
   {
     const double tr = my_pr * cr - my_pi * ci, ti = my_pr * ci + my_pi * cr;
     cr = tr;
