@@ -96,6 +96,34 @@ struct Launch {
   bool final_tt[2] = {false, false};    // 3-D final pass on the first section of `tt`
 };
 
+// Step kernels that begin with pdl_entry() are launched with programmatic
+// dependent launch allowed: their blocks are placed while the previous kernel
+// of the stream drains and wait on the device for its completion, so the gap
+// between the dozen short kernels of a step shrinks. NLS_PDL=0 launches them
+// plainly.
+bool pdl_on() {
+  static int v = [] {
+    const char *e = std::getenv("NLS_PDL");
+    return (e && std::atoi(e) == 0) ? 0 : 1;
+  }();
+  return v != 0;
+}
+template <typename K>
+cudaError_t pdl_launch(K kernel, dim3 grid, dim3 block, cudaStream_t st, const StepArgs &a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_on() ? 1 : 0;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, a);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <typename E, int SRC, bool HC>
 cudaError_t launch2_first(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_first<E, SRC, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
@@ -143,11 +171,8 @@ cudaError_t launch2_lanczos1_f32c(const StepArgs &a, int tiles, cudaStream_t st)
     const char *e = std::getenv("NLS_F32C_BLOCKS");
     return (e && std::atoi(e) == 5) ? 5 : 4;
   }();
-  if (minb == 5)
-    k2_lanczos1_f32c<5><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  else
-    k2_lanczos1_f32c<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
+  if (minb == 5) return pdl_launch(k2_lanczos1_f32c<5>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
+  return pdl_launch(k2_lanczos1_f32c<4>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 // Packed complex64 pass (NLSE, c == 1); NLS_C32=0 selects the generic
 // one-sequence complex pass, NLS_C32=3 the build for three blocks per SM.
@@ -160,19 +185,14 @@ int c32_mode() {
   return v;
 }
 cudaError_t launch2_lanczos1_c32(const StepArgs &a, int tiles, cudaStream_t st) {
-  if (c32_mode() == 3)
-    k2_lanczos1_c32<3><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  else
-    k2_lanczos1_c32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
+  if (c32_mode() == 3) return pdl_launch(k2_lanczos1_c32<3>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
+  return pdl_launch(k2_lanczos1_c32<4>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 cudaError_t launch2_first_c32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k2_first_c32<<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k2_first_c32, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 cudaError_t launch2_lanczos1_f32c_lo(const StepArgs &a, int tiles, cudaStream_t st) {
-  k2_lanczos1_f32c<4, true><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k2_lanczos1_f32c<4, true>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 cudaError_t launch2_lanczos1_f32b(const StepArgs &a, int tiles, cudaStream_t st) {
   if (f32_minb() == 3)
@@ -191,8 +211,7 @@ bool f32_first_packed() {
   return v != 0;
 }
 cudaError_t launch2_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k2_first_f32<<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k2_first_f32, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 cudaError_t launch2t_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   k2t_lanczos_f32<<<tiles, 128, sizeof(TmaSmem), st>>>(a);
@@ -212,8 +231,7 @@ bool use_tma() {
 }
 template <typename E, int NSEQ, int FIN, bool HC>
 cudaError_t launch2_final(const StepArgs &a, int tiles, cudaStream_t st) {
-  k2_final<E, NSEQ, FIN, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k2_final<E, NSEQ, FIN, HC>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 template <typename R, bool HC>
 cudaError_t launch2_sv(const StepArgs &a, int tiles, cudaStream_t st) {
@@ -274,24 +292,17 @@ bool ftri_smem_only() {
 template <typename E> cudaError_t launch_ftri(const StepArgs &a, int nslots_cap, cudaStream_t st) {
   const int warps = nslots_cap * a.nseq;
   const int blocks = (warps + 3) / 4;
-  if (ftri_smem_only() || a.k > 16)
-    k_ftri<E><<<blocks, 128, 0, st>>>(a);
-  else if (a.k <= 8)
-    k_ftri_reg<E, 8><<<blocks, 128, 0, st>>>(a);
-  else if (a.k <= 12)
-    k_ftri_reg<E, 12><<<blocks, 128, 0, st>>>(a);
-  else
-    k_ftri_reg<E, 16><<<blocks, 128, 0, st>>>(a);
-  return cudaGetLastError();
+  if (ftri_smem_only() || a.k > 16) return pdl_launch(k_ftri<E>, blocks, 128, st, a);
+  if (a.k <= 8) return pdl_launch(k_ftri_reg<E, 8>, blocks, 128, st, a);
+  if (a.k <= 12) return pdl_launch(k_ftri_reg<E, 12>, blocks, 128, st, a);
+  return pdl_launch(k_ftri_reg<E, 16>, blocks, 128, st, a);
 }
 template <typename E, int KIND>
 cudaError_t launch_ring(const StepArgs &a, int blocks_per_slot, int nslots_cap, cudaStream_t st) {
-  k_ring<E, KIND><<<dim3(blocks_per_slot, nslots_cap), 256, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k_ring<E, KIND>, dim3(blocks_per_slot, nslots_cap), 256, st, a);
 }
 cudaError_t launch_advance(const StepArgs &a, int nslots_cap, cudaStream_t st) {
-  k_advance<<<(nslots_cap + 127) / 128, 128, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k_advance, (nslots_cap + 127) / 128, 128, st, a);
 }
 
 // Kernel table of one (method family, dim, precision).

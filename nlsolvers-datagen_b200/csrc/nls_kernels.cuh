@@ -534,6 +534,7 @@ __device__ inline void fval(int fk, double lam, double tr, double ti, double &fr
 // capped (60); a slot that does not converge gets status NLS_ERR_NUMERIC.
 template <typename E>
 __global__ void __launch_bounds__(128) k_ftri(StepArgs a) {
+  pdl_entry();
   constexpr bool CP = Traits<E>::cplx;
   using R = typename Traits<E>::R;
   const int lane = threadIdx.x & 31;
@@ -929,6 +930,7 @@ __device__ bool ftri_fast(int k, const double *d, const double *e, int lane, int
 // synchronisation.
 template <typename E, int KP>
 __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
+  pdl_entry();
   constexpr bool CP = Traits<E>::cplx;
   using R = typename Traits<E>::R;
   const int lane = threadIdx.x & 31;

@@ -346,6 +346,7 @@ __host__ __device__ inline long long ring_count(int dim, int nx, int ny, int nz)
 template <typename E, int KIND>
 __global__ void __launch_bounds__(256) k_ring(StepArgs a) {
   using R = typename Traits<E>::R;
+  pdl_entry();
   if ((int)blockIdx.y >= *a.nslot_list) return;
   const int slot = a.slot_list[blockIdx.y];
   const SlotDesc &s = a.slots[slot];
@@ -380,6 +381,7 @@ __global__ void __launch_bounds__(256) k_ring(StepArgs a) {
 }
 
 static __global__ void k_advance(StepArgs a) {
+  pdl_entry();
   const int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= *a.nslot_list) return;
   a.state[a.slot_list[li]].step += 1;

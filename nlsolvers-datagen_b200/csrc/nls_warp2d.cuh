@@ -782,6 +782,7 @@ template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
 // measured faster than three blocks at 167 registers.
 template <typename E, int NSEQ, int FIN, bool HC>
 __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 1) k2_final(StepArgs a) {
+  pdl_entry();
   using R = typename Traits<E>::R;
   using FR = FinRow<FIN, E>;
   constexpr int NB = 8;
@@ -1652,6 +1653,7 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
 
 template <int MINB, bool LO = false>
 __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
+  pdl_entry();
   using E = float;
   __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
   WARP_TILE_PROLOGUE
@@ -1822,6 +1824,7 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
 }
 
 static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
+  pdl_entry();
   using E = float;
   WARP_TILE_PROLOGUE
   const int sq = t.local & 1;

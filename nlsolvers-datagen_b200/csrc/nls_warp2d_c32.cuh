@@ -156,6 +156,7 @@ __device__ __forceinline__ void lz1c32_cp_march(const float *pA, const float *pB
 
 template <int MINB>
 __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_c32(StepArgs a) {
+  pdl_entry();
   using E = Cx<float>;
   __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
   WARP_TILE_PROLOGUE
@@ -303,6 +304,7 @@ __device__ __forceinline__ void first_c32_march(const float *pU, const float *pM
 }
 
 static __global__ void __launch_bounds__(32 * WPB) k2_first_c32(StepArgs a) {
+  pdl_entry();
   using E = Cx<float>;
   WARP_TILE_PROLOGUE
   const int sq = t.local & 1;
