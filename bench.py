@@ -13,8 +13,9 @@ Inputs are seeded synthetic fields (kink/Gaussian mixtures, m = 1 + 0.2 GRF).
 N > 1 (torchrun, one process per GPU): every rank steps its own 64 trajectories
 (weak scaling, no data-path collective); the step time is the max over ranks.
 --impl reference times the reference algorithm's CPU restatement (the FP64
-oracle; the reference itself has no CPU path and cannot be built here) on the
-host cores, rank 0 only.
+oracle; the reference itself has no CPU path) on the host cores, rank 0 only,
+and reports beside it the reference's own per-trajectory FP64 GPU path,
+compiled from its sources, on one trajectory of the same grid.
 """
 from __future__ import annotations
 
@@ -214,6 +215,32 @@ def cpu_oracle_rate(cases, budget_s=12.0):
     return spec.n * steps / dt, steps, dt, O.num_threads()
 
 
+def reference_device_path(steps=50):
+    """The reference's own per-trajectory FP64 GPU path (device/include/
+    kg_single.cuh step with its cuBLAS/cuSPARSE/cuSOLVER Lanczos matrix
+    functions), compiled from its sources into oracle/_ref where the reference
+    checkout was present at build time: one trajectory of the batch's 300^2
+    grid (the reference steps trajectories one at a time), dt = 0.005, k = 10,
+    `steps` steps timed with CUDA events around its step loop after a short
+    warm-up run. Reported beside the CPU baseline, not as the line's value."""
+    from oracle import ref_kg
+    if not ref_kg.available():
+        return {"unavailable": "oracle/_ref/libref_kg.so not built (needs the reference checkout at build time)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+        gpu = torch.cuda.get_device_name(0)
+    except Exception as ex:  # torch without CUDA
+        return {"unavailable": f"no GPU ({ex})"}
+    for nt in (3, steps + 1):  # a warm-up run, then the timed run
+        spec, u0, v0, m, _ = make_batch(1, 0, 10, nt=nt, ns=1, T=nt * 0.005)[0]
+        _, _, ms = ref_kg.run(spec, u0, np.zeros_like(u0), m, 0)
+    return {"value": spec.n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "dtype": "f64",
+            "gpu": gpu, "workload": f"one 300^2 trajectory of the batch, dt=0.005, k=10, {steps} steps",
+            "source": "device/include/kg_single.cuh step compiled from the reference's sources (oracle/_ref)"}
+
+
 def run_reference(args, ws, rank, budget_s=150.0):
     """--impl reference: the FP64 CPU restatement of the reference algorithm
     (its own k = 10 for kg_gautschi_2d_dev). One step = one time step of the
@@ -222,6 +249,12 @@ def run_reference(args, ws, rank, budget_s=150.0):
     fewer. Under torchrun only rank 0 runs."""
     if rank != 0:
         return 0
+    # the reference's device path first: its step is bound by host round trips,
+    # so it is timed before the oracle's OpenMP threads occupy the host cores
+    try:
+        dev = reference_device_path()
+    except Exception as ex:  # reported, never fatal to the CPU line
+        dev = {"unavailable": f"{type(ex).__name__}: {ex}"}
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle import oracle as O
     from parity_util import oracle_problem
@@ -262,6 +295,7 @@ def run_reference(args, ws, rank, budget_s=150.0):
                          "sample": f"{args.steps} timed steps of {B} of the 64 trajectories (FP64, CGS re-orthogonalisation, OpenMP over grid points)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line["reference_device_path"] = dev
     print(json.dumps(line), flush=True)
     return 0
 
