@@ -8,7 +8,8 @@
 //                              the tile plus a one-cell halo from V_{j-1} (two-cell
 //                              halo) and V_{j-2}, store V_j, z_j = A v_j, dots
 //   f(T) kernel              : one warp per (slot, sequence): finish the scalars,
-//                              QL eigensolve of the k x k matrix, f(T) e1
+//                              f(T) e1 of the k x k matrix (Taylor series with a
+//                              rank-one correction, QL eigensolve as the fallback)
 //   final pass               : y = sum_j W_j V_j + Lam A V_{k-2} fused with the
 //                              integrator update and the snapshot write
 //   ghost-ring kernel        : Neumann ghost copies (boundaries.cuh:9-81)
