@@ -231,15 +231,20 @@ int nls_set_device(int32_t device);
    noise). All working memory is one static device array of
    NLS_NOALLOC_SCRATCH_BYTES per device; a grid that needs more (about
    (20 + 8(k-1)) bytes per padded point in FP32, twice that in FP64) is
-   rejected with NLS_ERR_CAPACITY, whose message gives both sizes. The call
-   allocates nothing, issues no host-to-device copy and returns after the
-   steps completed on `stream` (a cudaStream_t; NULL: the legacy stream).
-   The first call on a device does the set-up (loads the kernels and looks up
-   the scratch address); make it before any stream capture. Every call
-   re-initialises what must start at zero (reduction tickets, step state), so
-   nothing needs clearing between calls. All calls on one device share the
-   scratch: calls that overlap in time (from several threads or streams) race
-   and must be serialised by the caller. */
+   rejected with NLS_ERR_CAPACITY, whose message gives both sizes;
+   first_step + nsteps must stay below INT32_MAX. The call allocates nothing
+   and issues no host-to-device copy. It launches its kernels on `stream` (a
+   cudaStream_t; NULL: the legacy stream), then copies one device status word
+   to the host and synchronises `stream`, and returns after the steps
+   completed. The first call on a device does the set-up (loads the kernels
+   and looks up the scratch address); make that first call before any stream
+   capture. Every call re-initialises what must start at zero (reduction
+   tickets, step state), so nothing needs clearing between calls. All calls on
+   one device share the scratch: calls that overlap in time (from several
+   threads or streams) race and must be serialised by the caller. On
+   NLS_ERR_NUMERIC (non-finite Lanczos coefficients, or an eigensolver that
+   did not converge) u and u_past already hold the stepped, possibly invalid,
+   state. */
 #define NLS_NOALLOC_SCRATCH_BYTES (32u << 20)
 int nls_gautschi_step_noalloc(const nls_problem *p, double *u, double *u_past, const double *m,
                               const double *c, int32_t first_step, int32_t nsteps, void *stream);

@@ -6,13 +6,20 @@
 // the reference's device state (u, u_past, m: KGESolverDevice, kg_dev.hpp:32-131)
 // in place. All working memory (compensated fields, Krylov basis, reduction
 // partials, per-trajectory scalars, tile tables) lives in one file-scope
-// static __device__ array. The same step kernels as the pool engine run on it,
-// with the same launch sequence; descriptors and tile tables are written by a
-// set-up kernel from its parameters, so the call makes no allocation and no
-// host-to-device copy.
+// static __device__ array. The step is the pool engine's arithmetic through a
+// shorter launch sequence of its generic kernels: k2_first (one warp per
+// strip and sequence), the Lanczos passes k2_lanczos1_f32<4> (FP32, c == 1)
+// or k2_lanczos1 (FP64, or with a c field), f(T)e1 by the shared-memory QL
+// solve k_ftri, then k2_final, k_ring and k_advance. The pool's defaults
+// (k2_lanczos1_f32c, the packed first pass and the Taylor f(T) of
+// k_ftri_reg) are not used, so results agree with the pool within the
+// precision's tolerance, not bitwise. Descriptors and tile tables are written
+// by a set-up kernel from its parameters, so the call makes no allocation and
+// no host-to-device copy.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -223,8 +230,11 @@ int run(const nls_problem &p, double *u, double *u_past, const double *m, const 
   sd.r0 = p.r0;
   sd.seed = p.seed;
   sd.nt = p.nt;
-  sd.ns = 1;
-  sd.freq = 0x7fffffff;  // no snapshot step
+  // No snapshot at any step: with ns = 0 the cadence test (snap_step) fails
+  // for every step index, including 0, so no kernel touches a snapshot frame
+  // (this path has none).
+  sd.ns = 0;
+  sd.freq = 0x7fffffff;
   sd.snap_frames = 1;
   sd.n = (int64_t)p.nx * p.ny;
   sd.active = 1;
@@ -304,7 +314,10 @@ int run(const nls_problem &p, double *u, double *u_past, const double *m, const 
   int status = 0;
   CKN(cudaMemcpyAsync(&status, &((SlotState *)(base + L.state))->status, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKN(cudaStreamSynchronize(st));
-  if (status) return fail(NLS_ERR_NUMERIC, "the tridiagonal eigensolver did not converge");
+  // Status words as the pool engine reports them (nls_pool_sync).
+  if (status == -9)
+    return fail(NLS_ERR_NUMERIC, "diverged: non-finite Lanczos coefficients (u and u_past hold the stepped state)");
+  if (status) return fail(NLS_ERR_NUMERIC, "the tridiagonal eigensolver did not converge (u and u_past hold the stepped state)");
   return NLS_OK;
 }
 
@@ -327,6 +340,9 @@ extern "C" int nls_gautschi_step_noalloc(const nls_problem *p, double *u, double
     return fail(NLS_ERR_INVALID_ARG, "precision must be NLS_FP32 or NLS_FP64");
   if (!(p->T > 0.0) || p->nt <= 0) return fail(NLS_ERR_INVALID_ARG, "need T > 0 and nt > 0 (dt = T/nt)");
   if (nsteps < 0 || first_step < 0) return fail(NLS_ERR_INVALID_ARG, "negative step count");
+  // The device step counter is an int that runs up to first_step + nsteps.
+  if ((int64_t)first_step + (int64_t)nsteps > (int64_t)INT32_MAX - 1)
+    return fail(NLS_ERR_INVALID_ARG, "first_step + nsteps exceeds the step counter's range");
   const int64_t need = scratch_needed(p);
   if (need < 0 || need > (int64_t)NLS_NOALLOC_SCRATCH_BYTES)
     return fail(NLS_ERR_CAPACITY, "grid needs " + std::to_string(need) + " bytes of scratch; the static scratch holds " +

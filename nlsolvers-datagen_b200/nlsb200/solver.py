@@ -88,11 +88,6 @@ class Spec:
         p.nonlinearity = self.nonlinearity
         return p
 
-    def oracle_params(self):
-        """Nonlinearity coefficients as the library resolves them."""
-        s = self.struct(False)
-        return dict(k=s.k, p1=s.p1, q1=s.q1, p3=s.p3, q3=s.q3, rm=s.rm, r0=s.r0, nonlinearity=s.nonlinearity)
-
 
 def reference_phi4_rm(spec: Spec) -> float:
     """-alpha sqrt(kBT dx)/dt with alpha = 0.01, kBT = 2, dx = 2L/(nx-1)

@@ -4,12 +4,18 @@ initial conditions and coefficient fields with numpy, e.g.
 scripts/real_launcher_2d.py:78-124).
 
 Grid coordinates follow the drivers: x_i = -L + i dx, dx = 2L/(n-1).
+
+The field generators use numpy only and this module imports nothing else at
+load time, so a caller that must not load the engine (the CPU baseline of the
+benchmark) can load this file on its own and call kg_fields / nlse_fields; the
+*_case helpers add the engine's Spec.
 """
 from __future__ import annotations
 
 import numpy as np
 
-from .solver import FP32, KG_GAUTSCHI, NLSE_SS2, Spec
+# integrator and precision codes (include/nlsb200.h)
+KG_GAUTSCHI, NLSE_SS2, FP32 = 0, 4, 0
 
 
 def axes(dim, n, L):
@@ -81,26 +87,38 @@ def nlse_solitons(dim, n, L, rng):
     return u
 
 
-def kg_case(n, L, T, nt, ns, k=10, seed=0, dim=2, method=KG_GAUTSCHI, precision=FP32,
-            kinks=False):
-    """(spec, u0, v0, m, c) for a KG / phi^4 trajectory with c == 1."""
+def kg_fields(n, L, seed=0, dim=2, kinks=False):
+    """(u0, v0, m, c) of a KG / phi^4 trajectory with c == 1 (numpy only)."""
     rng = np.random.default_rng(seed)
-    spec = Spec(method=method, dim=dim, nx=n, ny=n, nz=n if dim == 3 else 1, Lx=L, Ly=L, Lz=L,
-                T=T, nt=nt, ns=ns, k=k, precision=precision, seed=seed)
     u0 = kink_mix(n, L, rng) if kinks else gaussian_bumps(dim, n, L, rng, centre=0.6 * L)
     v0 = np.zeros_like(u0)
     m = mass_field(u0.shape, rng)
     c = np.ones_like(u0)
+    return u0, v0, m, c
+
+
+def nlse_fields(n, L, seed=0, dim=2):
+    """(u0, m, c) of an NLSE trajectory with m == c == 1 (numpy only)."""
+    rng = np.random.default_rng(seed)
+    u0 = nlse_solitons(dim, n, L, rng)
+    return u0, np.ones(u0.shape), np.ones(u0.shape)
+
+
+def kg_case(n, L, T, nt, ns, k=10, seed=0, dim=2, method=KG_GAUTSCHI, precision=FP32,
+            kinks=False):
+    """(spec, u0, v0, m, c) for a KG / phi^4 trajectory with c == 1."""
+    from .solver import Spec
+    spec = Spec(method=method, dim=dim, nx=n, ny=n, nz=n if dim == 3 else 1, Lx=L, Ly=L, Lz=L,
+                T=T, nt=nt, ns=ns, k=k, precision=precision, seed=seed)
+    u0, v0, m, c = kg_fields(n, L, seed, dim, kinks)
     return spec, u0, v0, m, c
 
 
 def nlse_case(n, L, T, nt, ns, k=12, seed=0, dim=2, method=NLSE_SS2, precision=FP32):
-    rng = np.random.default_rng(seed)
+    from .solver import Spec
     spec = Spec(method=method, dim=dim, nx=n, ny=n, nz=n if dim == 3 else 1, Lx=L, Ly=L, Lz=L,
                 T=T, nt=nt, ns=ns, k=k, precision=precision, seed=seed)
-    u0 = nlse_solitons(dim, n, L, rng)
-    m = np.ones(u0.shape)
-    c = np.ones(u0.shape)
+    u0, m, c = nlse_fields(n, L, seed, dim)
     return spec, u0, None, m, c
 
 

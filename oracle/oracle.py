@@ -202,6 +202,34 @@ class Problem:
         return s
 
 
+def reference_coefficients(method, dim, nx, Lx, dt):
+    """The reference's equation coefficients and default Krylov dimension per
+    executable, written out here from its sources (not taken from the
+    product library) so that a wrong default in the product cannot pass
+    unseen:
+      KG Gautschi / SV: g(u) = -m u^3               (kg_single.cuh:105-108, :152-155)
+      phi^4 SV:         g(u) = -m (u - u^3 + s xi)  (stochastic_phi4.cuh:52),
+                        s = 0.01 sqrt(2 dx) / dt    (stochastic_phi4_dev.hpp:47-51)
+      NLSE:             rho = m |u|^2               (nlse_dev.hpp:20-29)
+      k: KG / phi^4 10 (kg_driver_dev_2d.cpp:138, sp4_sv_driver_dev_2d.cpp:135),
+         SS2 2-D 20 / 3-D 25 (nlse_cubic_driver_2d.cpp:104, nlse_cubic_driver_3d.cpp:112),
+         SEWI 2-D 10 / 3-D 15 (nlse_cubic_sewi_driver_2d.cpp:104, _3d.cpp:112).
+    In the oracle's form g(u) = (p1 m + q1) u + (p3 m + q3) u^3 + (rm m + r0) xi."""
+    c = dict(p1=0.0, q1=0.0, p3=0.0, q3=0.0, rm=0.0, r0=0.0, nonlinearity=0)
+    if method in (KG_GAUTSCHI, KG_SV):
+        c.update(p3=-1.0, k=10)
+    elif method in (SP4_SV, SP4_GAUTSCHI):
+        dx = 2.0 * Lx / (nx - 1)
+        c.update(p1=-1.0, p3=1.0, rm=-(0.01 * np.sqrt(2.0 * dx) / dt), k=10)
+    elif method == NLSE_SS2:
+        c.update(p3=1.0, k=20 if dim == 2 else 25)
+    elif method == NLSE_SEWI:
+        c.update(p3=1.0, k=10 if dim == 2 else 15)
+    else:
+        raise ValueError(f"unknown method {method}")
+    return c
+
+
 def run(prob: Problem, u0, v0, m, c):
     """Full driver run; returns (traj, vel) shaped (ns, *grid) (vel None for NLSE)."""
     cplx = prob.method in (NLSE_SS2, NLSE_SEWI)

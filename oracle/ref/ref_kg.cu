@@ -1,5 +1,6 @@
-// Runs the reference's own device code for the KG integrators, compiled from
-// its sources (device/include/kg_single.cuh: step, step_sv; matfunc_real.hpp,
+// Runs the reference's own device code for the KG integrators and the phi^4
+// step, compiled from its sources (device/include/kg_single.cuh: step,
+// step_sv; stochastic_phi4.cuh: SP4Solver::step; matfunc_real.hpp,
 // lanczos.hpp, spmv.hpp: the Lanczos matrix functions; boundaries.cuh:
 // neumann_bc_no_velocity_blocking and its 3-D form). Test infrastructure: the
 // tests compare the oracle and the engine with it.
@@ -10,10 +11,16 @@
 // kg_dev.hpp:116-121, the device-side snapshot store of kg_dev.hpp:123-131
 // (transferred once at the end, kg_dev.hpp:107-114) and the driver loop of
 // kg_driver_dev_2d.cpp:144-153 (step, boundary copy, snapshot every nt/ns
-// steps). If loop_ms is not null it receives the duration of that loop (CUDA
-// events on the default stream, which all of the reference's work uses). The caller passes the operator as
-// CSR arrays (A = -L for Gautschi, L for Stormer-Verlet,
-// kg_driver_dev_2d.cpp:105-108, kg_sv_driver_dev_2d.cpp:102-105), since the
+// steps). The phi^4 solver class (stochastic_phi4_dev.hpp:29-133) and its
+// driver loop (sp4_sv_driver_dev_2d.cpp:135-151) have the same structure and
+// are restated the same way; its step takes the noise strength as an argument
+// (stochastic_phi4.cuh:22-24), which the caller passes (0: deterministic, as
+// the noise term is then 0 * N(0,1) = 0 at every point). If loop_ms is not
+// null it receives the duration of that loop (CUDA events on the default
+// stream, which all of the reference's work uses). The caller passes the
+// operator as CSR arrays (A = -L for Gautschi, L for Stormer-Verlet and phi^4,
+// kg_driver_dev_2d.cpp:105-108, kg_sv_driver_dev_2d.cpp:102-105,
+// sp4_sv_driver_dev_2d.cpp:102-105), since the
 // reference assembles it with Eigen (laplacians.hpp). Square and cubic grids
 // only, as KGESolverDevice (kg_dev.hpp:38-45).
 #include <cstdint>
@@ -22,11 +29,13 @@
 
 #include "boundaries.cuh"
 #include "kg_single.cuh"
+#include "stochastic_phi4.cuh"
 
 extern "C" int ref_kg_run(int32_t dim, int32_t method, int32_t nx, const int32_t *row_ptr, const int32_t *col_ind,
                           const double *vals, int32_t nnz, int32_t k, const double *u0, const double *v0,
                           const double *m, double dt, int32_t nt, int32_t ns, double *traj, double *vel,
-                          double *loop_ms) {
+                          double *loop_ms, double sp4_scale) {
+  if (method < 0 || method > 2) return -3;
   if ((dim != 2 && dim != 3) || nx < 3 || k < 2 || nt < 1 || ns < 1 || nt < ns) return -3;
   const uint32_t n = (uint32_t)nx * (uint32_t)nx * (dim == 3 ? (uint32_t)nx : 1u);
   if (row_ptr[0] != 0 || row_ptr[n] != nnz) return -3;
@@ -64,8 +73,10 @@ extern "C" int ref_kg_run(int32_t dim, int32_t method, int32_t nx, const int32_t
     for (int i = 1; i < nt; ++i) {
       if (method == 0)
         device::KGESolver::step(d_v, d_u, d_up, d_b1, d_b2, d_b3, &matfunc, d_m, dt, n, grid, block);
-      else
+      else if (method == 1)
         device::KGESolver::step_sv(d_v, d_u, d_up, d_b1, d_b2, d_b3, &matfunc, d_m, dt, n, grid, block);
+      else
+        device::SP4Solver::step(d_v, d_u, d_up, d_b1, d_b2, d_b3, &matfunc, d_m, dt, n, sp4_scale, grid, block);
       if (dim == 2)
         neumann_bc_no_velocity_blocking<double>(d_u, e, e);
       else

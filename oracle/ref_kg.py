@@ -1,8 +1,9 @@
-"""ctypes front end of oracle/_ref/libref_kg.so: the reference's own KG device
-code (device/include/kg_single.cuh step / step_sv with the Lanczos matrix
-functions of matfunc_real.hpp and lanczos.hpp, the SpMV of spmv.hpp and the
-ghost copies of boundaries.cuh), compiled from its sources by oracle/Makefile
-with the driver oracle/ref/ref_kg.cu.
+"""ctypes front end of oracle/_ref/libref_kg.so: the reference's own KG and
+phi^4 device code (device/include/kg_single.cuh step / step_sv and
+stochastic_phi4.cuh SP4Solver::step, with the Lanczos matrix functions of
+matfunc_real.hpp and lanczos.hpp, the SpMV of spmv.hpp and the ghost copies of
+boundaries.cuh), compiled from its sources by oracle/Makefile with the driver
+oracle/ref/ref_kg.cu.
 
 TEST INFRASTRUCTURE ONLY: used by tests/ (to pin the oracle and the engine to
 the reference's code) and by bench.py's reference arm (to time the reference's
@@ -33,7 +34,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         ip, dp, i32 = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double), ctypes.c_int32
         L.ref_kg_run.argtypes = [i32, i32, i32, ip, ip, dp, i32, i32, dp, dp, dp, ctypes.c_double, i32, i32,
-                                 dp, dp, dp]
+                                 dp, dp, dp, ctypes.c_double]
         L.ref_kg_run.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -83,10 +84,12 @@ def csr(spec, sign):
     return indptr, indices, vals.astype(np.float64)
 
 
-def run(spec, u0, v0, m, method):
+def run(spec, u0, v0, m, method, sp4_scale=0.0):
     """One trajectory through the reference's code (method 0: Gautschi with
-    A = -L, 1: Stormer-Verlet with L): (traj, vel, step-loop ms). Square and
-    cubic grids only, as the reference's solver class (kg_dev.hpp:38-45)."""
+    A = -L, 1: Stormer-Verlet with L, 2: the phi^4 step with L and noise
+    strength sp4_scale, stochastic_phi4.cuh:19-77): (traj, vel, step-loop ms).
+    Square and cubic grids only, as the reference's solver classes
+    (kg_dev.hpp:38-45, stochastic_phi4_dev.hpp:37-44)."""
     L = lib()
     indptr, indices, vals = csr(spec, -1.0 if method == 0 else 1.0)
     traj = np.zeros((spec.ns,) + spec.shape)
@@ -97,7 +100,7 @@ def run(spec, u0, v0, m, method):
     ms = ctypes.c_double(0.0)
     rc = L.ref_kg_run(spec.dim, method, spec.nx, pi(indptr), pi(indices), pd(vals), len(vals), spec.k,
                       pd(args[0]), pd(args[1]), pd(args[2]), spec.dt, spec.nt, spec.ns, pd(traj), pd(vel),
-                      ctypes.byref(ms))
+                      ctypes.byref(ms), float(sp4_scale))
     if rc != 0:
         raise RuntimeError(f"reference KG run failed: {rc}")
     return traj, vel, ms.value

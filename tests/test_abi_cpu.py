@@ -50,6 +50,26 @@ def test_problem_defaults_match_reference_binaries(nl):
     assert (p.p1, p.p3) == (-1.0, 1.0)  # -m (u - u^3 + s xi)
 
 
+def test_product_defaults_equal_oracle_restatement(nl):
+    """Every method's coefficients and k, as the product resolves them for a
+    Spec that sets none (nls_problem_defaults plus the phi^4 noise scale),
+    equal the oracle's own restatement of the reference
+    (oracle.reference_coefficients), including the NLSE p3 = 1."""
+    from oracle import oracle as O
+    for method in (nl.KG_GAUTSCHI, nl.KG_SV, nl.SP4_SV, nl.SP4_GAUTSCHI, nl.NLSE_SS2, nl.NLSE_SEWI):
+        for dim in (2, 3):
+            spec = nl.Spec(method=method, dim=dim, nx=41, ny=41, nz=41 if dim == 3 else 1, Lx=7.0, Ly=7.0,
+                           Lz=7.0, T=0.3, nt=60, ns=3)
+            p = spec.struct(False)
+            want = O.reference_coefficients(method, dim, spec.nx, spec.Lx, spec.dt)
+            got = dict(k=p.k, p1=p.p1, q1=p.q1, p3=p.p3, q3=p.q3, r0=p.r0, nonlinearity=p.nonlinearity)
+            for key, v in got.items():
+                assert v == want[key], (method, dim, key, v, want[key])
+            assert p.rm == pytest.approx(want["rm"], rel=1e-15, abs=0), (method, dim)
+    p = nl.Spec(method=nl.NLSE_SS2, dim=2, nx=8, ny=8).struct(False)
+    assert p.p3 == 1.0  # rho = m |u|^2 (nlse_dev.hpp:27)
+
+
 def test_phi4_noise_scale(nl):
     spec = nl.Spec(method=nl.SP4_SV, dim=2, nx=101, ny=101, Lx=10, Ly=10, T=1.0, nt=100, ns=10)
     dx = 20 / 100
