@@ -3,23 +3,30 @@
 
 Workload (the headline batched configuration): 64 nonlinear Klein-Gordon
 trajectories u_tt = Lap u - m u^3 on [-15,15]^2, 300 x 300 grid (incl. ghost
-ring), Gautschi step with a k-step Lanczos cos / sinc^2 filter (k picked by the
-project autotuner in 8..16), dt = 0.005, nt = 6000, 50 snapshots, FP32 Krylov
-basis + compensated FP32 fields. A "step" is one time step of the whole batch.
+ring), Gautschi step with a k-step Lanczos cos / sinc^2 filter, dt = 0.005,
+nt = 6000, 50 snapshots, FP32 Krylov basis + compensated FP32 fields. k = 9:
+the project autotuner's choice for this workload (the smallest k in 8..16
+whose 10-step result stays within 5e-6 of k = 24), re-checked live and
+reported under "tuning". A "step" is one time step of the whole batch.
 Inputs are seeded synthetic fields (kink/Gaussian mixtures, m = 1 + 0.2 GRF).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 (torchrun, one process per GPU): every rank steps its own 64 trajectories
-(weak scaling, no data-path collective); the step time is the max over ranks.
+N > 1: one process per GPU (started here through torch.distributed.run when
+WORLD_SIZE is unset); every rank steps its own 64 trajectories (weak scaling,
+no data-path collective); the step time is the max over ranks.
+The timed region is repeated in blocks of exactly K steps until it lasts about
+a second (clock samples); the line reports the median block.
 --impl reference times the reference algorithm's CPU restatement (the FP64
 oracle; the reference itself has no CPU path) on the host cores, rank 0 only,
-and reports beside it the reference's own per-trajectory FP64 GPU path,
-compiled from its sources, on one trajectory of the same grid.
+with the same k and configuration, and reports beside it the reference's own
+per-trajectory FP64 GPU path, compiled from its sources, on one trajectory of
+the same grid. That arm imports nothing of the engine.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import statistics
@@ -39,7 +46,21 @@ import numpy as np  # noqa: E402
 METRIC = "grid-point-steps/s batched FP32 vs plain FP64 @rel-L2≤1e-5; HBM GB/s; p50/p99"
 UNIT = "grid-point-steps/s"
 CFG = dict(n=300, L=15.0, T=30.0, nt=6000, ns=50, batch=64)
+K_HEADLINE = 9
 FALLBACK_HBM = 6650.0
+# DRAM bytes (read + write) per grid point of one Lanczos pass launch
+# (k2_lanczos1_f32c, j = 2, both sequences) in the ncu capture of
+# profiles/ncu_lanczos_pass_kg2d.md; algorithmic: 24 B per point.
+TRAFFIC_BYTES_PER_POINT_PASS = 17.85
+TIMED_REGION_S = 1.0
+
+
+def workload_config(k, ws, B):
+    """The configuration both arms report (identical keys and values)."""
+    return {"workload": "KG 2-D Gautschi batch, 64 x 300^2 on [-15,15]^2, dt=0.005, nt=6000, ns=50",
+            "global_batch": B * ws, "per_gpu_batch": B, "grid": [CFG["n"], CFG["n"]], "k": k,
+            "parallelism": f"trajectory shards x{ws}",
+            "l2": "working set 0.6 GB per GPU >> 126 MB L2 (no flush needed)"}
 
 
 def hbm_peak():
@@ -144,15 +165,55 @@ class Clocks:
                 "samples": len(self.rows), "source": f"NVML every 2 ms ({self.device})"}
 
 
-def make_batch(B, rank, k, nt=None, ns=None, T=None):
-    from nlsb200 import workloads as W
-    cases = []
+_FIELDS = None
+
+
+def fields_module():
+    """nlsb200/workloads.py loaded on its own (numpy only, no engine import),
+    so that the reference arm builds the same inputs without the engine."""
+    global _FIELDS
+    if _FIELDS is None:
+        path = os.path.join(PKG, "nlsb200", "workloads.py")
+        spec = importlib.util.spec_from_file_location("nls_bench_fields", path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _FIELDS = mod
+    return _FIELDS
+
+
+def batch_fields(B, rank):
+    """(seed, u0, v0, m, c) of the batch's trajectories on `rank`: seed
+    1000 rank + i, kink mixtures for even i."""
+    F = fields_module()
+    out = []
     for i in range(B):
-        spec, u0, v0, m, c = W.kg_case(CFG["n"], CFG["L"], T or CFG["T"], nt or CFG["nt"],
-                                       ns or CFG["ns"], k=k, seed=1000 * rank + i,
-                                       kinks=(i % 2 == 0))
+        seed = 1000 * rank + i
+        out.append((seed,) + F.kg_fields(CFG["n"], CFG["L"], seed=seed, kinks=(i % 2 == 0)))
+    return out
+
+
+def make_batch(B, rank, k, nt=None, ns=None, T=None):
+    """The batch as engine problems: (Spec, u0, v0, m, c) per trajectory."""
+    from nlsb200.solver import FP32, KG_GAUTSCHI, Spec
+    cases = []
+    for seed, u0, v0, m, c in batch_fields(B, rank):
+        spec = Spec(method=KG_GAUTSCHI, dim=2, nx=CFG["n"], ny=CFG["n"], Lx=CFG["L"], Ly=CFG["L"], Lz=CFG["L"],
+                    T=T or CFG["T"], nt=nt or CFG["nt"], ns=ns or CFG["ns"], k=k, precision=FP32, seed=seed)
         cases.append((spec, u0, v0, m, c))
     return cases
+
+
+def oracle_problem(k, seed=0, nt=None, ns=None, T=None):
+    """The FP64 oracle's problem for one trajectory of the workload, with the
+    reference's KG coefficients (oracle.reference_coefficients); no engine
+    import."""
+    from oracle import oracle as O
+    nt, ns, T = nt or CFG["nt"], ns or CFG["ns"], T or CFG["T"]
+    prm = O.reference_coefficients(O.KG_GAUTSCHI, 2, CFG["n"], CFG["L"], T / nt)
+    return O.Problem(dim=2, nx=CFG["n"], ny=CFG["n"], nz=1, Lx=CFG["L"], Ly=CFG["L"], Lz=CFG["L"], T=T, nt=nt,
+                     ns=ns, k=k, method=O.KG_GAUTSCHI, sewi_variant=0, reorth=1, max_steps=0, p1=prm["p1"],
+                     q1=prm["q1"], p3=prm["p3"], q3=prm["q3"], rm=prm["rm"], r0=prm["r0"], seed=seed,
+                     nonlinearity=0)
 
 
 def dist_init():
@@ -195,34 +256,55 @@ def barrier(ws):
         dist.barrier()
 
 
-def cpu_oracle_rate(cases, budget_s=12.0):
-    """FP64 oracle (C++/OpenMP restatement of the reference) on one trajectory of
-    the batch for a bounded number of pure steps; returns gp-steps/s."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
+def kg_energy(u, v, m):
+    from oracle import diagnostics as D
+    e = D.kg(u, v, m, np.ones_like(u), (CFG["L"], CFG["L"]))
+    return float(e[0] + e[1] + e[2])
+
+
+def cpu_parity_leg(k, traj, vel):
+    """The FP64 oracle (C++/OpenMP restatement of the reference) runs
+    trajectory 0 of the batch through the whole job (5999 steps, 50
+    snapshots). Its wall time is the CPU baseline; its snapshots are the
+    parity reference for the same trajectory of the end-to-end job (traj, vel:
+    that job's snapshots of trajectory 0)."""
     from oracle import oracle as O
-    from parity_util import oracle_problem
-    spec, u0, v0, m, c = cases[0]
-    st = O.RealStepper(oracle_problem(spec, reorth=True), u0, v0, m, c)
-    st.advance(1)
+    seed, u0, v0, m, c = batch_fields(1, 0)[0]
     t0 = time.perf_counter()
-    st.advance(2)
-    per = (time.perf_counter() - t0) / 2
-    steps = max(2, min(spec.nt - 4, int(budget_s / max(per, 1e-4))))
-    t0 = time.perf_counter()
-    st.advance(steps)
-    dt = time.perf_counter() - t0
-    st.close()
-    return spec.n * steps / dt, steps, dt, O.num_threads()
+    otraj, ovel = O.run(oracle_problem(k, seed=seed), u0, v0, m, c)
+    secs = time.perf_counter() - t0
+    steps = CFG["nt"] - 1
+    rate = CFG["n"] ** 2 * steps / secs
+    errs = [float(np.linalg.norm(traj[i] - otraj[i]) / np.linalg.norm(otraj[i])) for i in range(CFG["ns"])]
+    e0 = kg_energy(otraj[0], ovel[0], m)
+    parity = {"rel_l2_final": errs[-1], "rel_l2_max_snapshot": max(errs),
+              "energy_drift": abs(kg_energy(traj[-1], vel[-1], m) - e0) / abs(e0),
+              "energy_drift_oracle": abs(kg_energy(otraj[-1], ovel[-1], m) - e0) / abs(e0),
+              "traj": 0, "steps": steps, "k": k, "bound": 1e-5,
+              "against": "FP64 oracle (CGS re-orthogonalisation), final snapshot = state after step 5880"}
+    cpu = {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+           "sample": f"trajectory 0 of the batch, 300^2, the whole job ({steps} steps, 50 snapshots) in "
+                     f"{secs:.1f} s (FP64 oracle, CGS re-orthogonalisation, OpenMP over grid points)"}
+    return cpu, parity
 
 
-def reference_device_path(steps=50):
+def _ref_spec(k, nt, ns, T):
+    """The attributes oracle/ref_kg.py reads from a problem (no engine Spec)."""
+    from types import SimpleNamespace
+    n, L = CFG["n"], CFG["L"]
+    return SimpleNamespace(dim=2, nx=n, ny=n, nz=1, Lx=L, Ly=L, Lz=L, shape=(n, n), n=n * n, k=k, nt=nt, ns=ns,
+                           T=T, dt=T / nt)
+
+
+def reference_device_path(k, steps=50):
     """The reference's own per-trajectory FP64 GPU path (device/include/
     kg_single.cuh step with its cuBLAS/cuSPARSE/cuSOLVER Lanczos matrix
     functions), compiled from its sources into oracle/_ref where the reference
-    checkout was present at build time: one trajectory of the batch's 300^2
-    grid (the reference steps trajectories one at a time), dt = 0.005, k = 10,
-    `steps` steps timed with CUDA events around its step loop after a short
-    warm-up run. Reported beside the CPU baseline, not as the line's value."""
+    checkout was present at build time: trajectory 0 of the batch's 300^2 grid
+    (the reference steps trajectories one at a time), dt = 0.005, Krylov
+    dimension k, `steps` steps timed with CUDA events around its step loop
+    after a short warm-up run. Reported beside the CPU baseline, not as the
+    line's value."""
     from oracle import ref_kg
     if not ref_kg.available():
         return {"unavailable": "oracle/_ref/libref_kg.so not built (needs the reference checkout at build time)"}
@@ -233,37 +315,37 @@ def reference_device_path(steps=50):
         gpu = torch.cuda.get_device_name(0)
     except Exception as ex:  # torch without CUDA
         return {"unavailable": f"no GPU ({ex})"}
+    seed, u0, v0, m, c = batch_fields(1, 0)[0]
     for nt in (3, steps + 1):  # a warm-up run, then the timed run
-        spec, u0, v0, m, _ = make_batch(1, 0, 10, nt=nt, ns=1, T=nt * 0.005)[0]
-        _, _, ms = ref_kg.run(spec, u0, np.zeros_like(u0), m, 0)
+        spec = _ref_spec(k, nt, 1, nt * 0.005)
+        _, _, ms = ref_kg.run(spec, u0, v0, m, 0)
     return {"value": spec.n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "dtype": "f64",
-            "gpu": gpu, "workload": f"one 300^2 trajectory of the batch, dt=0.005, k=10, {steps} steps",
+            "gpu": gpu, "workload": f"trajectory 0 of the batch, 300^2, dt=0.005, k={k}, {steps} steps",
             "source": "device/include/kg_single.cuh step compiled from the reference's sources (oracle/_ref)"}
 
 
 def run_reference(args, ws, rank, budget_s=150.0):
-    """--impl reference: the FP64 CPU restatement of the reference algorithm
-    (its own k = 10 for kg_gautschi_2d_dev). One step = one time step of the
-    first B' trajectories of the batch (stateful, so no per-call setup is
-    timed); B' = 64 unless --steps would run past about budget_s seconds, then
-    fewer. Under torchrun only rank 0 runs."""
+    """--impl reference: the FP64 CPU restatement of the reference algorithm at
+    the same k and configuration as the engine's line. One step = one time
+    step of the first B' trajectories of the batch (stateful, so no per-call
+    setup is timed); B' = 64 unless --steps would run past about budget_s
+    seconds, then fewer. Under torchrun only rank 0 runs. Nothing of the
+    engine is imported: inputs come from the numpy-only field generators and
+    the coefficients from the oracle's restatement of the reference."""
     if rank != 0:
         return 0
+    k = K_HEADLINE
     # the reference's device path first: its step is bound by host round trips,
     # so it is timed before the oracle's OpenMP threads occupy the host cores
     try:
-        dev = reference_device_path()
+        dev = reference_device_path(k)
     except Exception as ex:  # reported, never fatal to the CPU line
         dev = {"unavailable": f"{type(ex).__name__}: {ex}"}
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle import oracle as O
-    from parity_util import oracle_problem
-    k = 10
-    cases = make_batch(CFG["batch"], 0, k)
-    n = cases[0][0].n
-    B = len(cases)
-    steppers = [O.RealStepper(oracle_problem(spec, reorth=True), u0, v0, m, c)
-                for spec, u0, v0, m, c in cases]
+    fields = batch_fields(CFG["batch"], 0)
+    n = CFG["n"] ** 2
+    B = len(fields)
+    steppers = [O.RealStepper(oracle_problem(k, seed=seed), u0, v0, m, c) for seed, u0, v0, m, c in fields]
 
     def one_step():
         t0 = time.perf_counter()
@@ -285,14 +367,14 @@ def run_reference(args, ws, rank, budget_s=150.0):
     total = sum(ts)
     value = B * n * args.steps / total
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded kink/Gaussian u0, m = 1 + 0.2 GRF(k^-3))",
-        "config": {"workload": "KG 2-D Gautschi batch, 64 x 300^2 on [-15,15]^2, dt=0.005, k=10",
-                   "global_batch": B, "grid": [CFG["n"], CFG["n"]], "k": k},
+        "config": workload_config(k, ws, CFG["batch"]),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                         "sample": f"{args.steps} timed steps of {B} of the 64 trajectories (FP64, CGS re-orthogonalisation, OpenMP over grid points)"},
+                         "sample": f"{args.steps} timed steps of {B} of the 64 trajectories (FP64, CGS "
+                                   "re-orthogonalisation, OpenMP over grid points)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     line["reference_device_path"] = dev
@@ -357,6 +439,24 @@ def run_small(args, lrank):
     return 0
 
 
+def timed_blocks(pool, steps, ws, target_s=TIMED_REGION_S, max_blocks=200):
+    """Blocks of exactly `steps` steps, each bracketed by a barrier and a device
+    sync and timed with CUDA events on the pool's stream (max over ranks),
+    repeated until they add up to about target_s; returns the block times."""
+    times = []
+    while True:
+        pool.sync()
+        barrier(ws)
+        ms = allreduce_max(pool.step_timed(steps), ws)
+        times.append(ms)
+        nblk = len(times)
+        if nblk >= max_blocks or bcast_int(int(sum(times) >= 1e3 * target_s), ws):
+            break
+    pool.sync()
+    barrier(ws)
+    return times
+
+
 def run_ours(args, ws, rank, lrank):
     import nlsb200 as nl
     from nlsb200 import autotune
@@ -366,16 +466,15 @@ def run_ours(args, ws, rank, lrank):
         return run_small(args, lrank)
     nl.lib().nls_set_device(lrank)
     B = CFG["batch"]
-    # k by the a-posteriori Krylov error estimate on rank 0's first trajectory
-    probe = make_batch(1, 0, 16)[0]
-    k = None
-    kreport = {}
+    k = K_HEADLINE
+    tuning = {}
     if rank == 0:
-        # the reference leaves T[k-1,k-1] = 0, so its result converges only
-        # algebraically in k; accept k when 10 probe steps stay within 5e-6 of k = 24
-        k, kreport = autotune.choose_k(*probe, candidates=tuple(range(8, 17)), k_ref=24,
-                                       steps=10, tol=5e-6)
-    k = bcast_int(k if k is not None else 0, ws)
+        # the live re-check of k: the reference leaves T[k-1,k-1] = 0, so its
+        # result converges only algebraically in k; the autotuner accepts k
+        # when 10 probe steps stay within 5e-6 of k = 24
+        probe = make_batch(1, 0, 16)[0]
+        k_auto, kreport = autotune.choose_k(*probe, candidates=tuple(range(8, 17)), k_ref=24, steps=10, tol=5e-6)
+        tuning.update({"k_autotune": k_auto, "k_autotune_err": kreport, "k_used": k})
     cases = make_batch(B, rank, k)
     n = cases[0][0].n
     cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
@@ -393,16 +492,15 @@ def run_ours(args, ws, rank, lrank):
     # = 2304 warps, one wave of 16 warps on each of the 148 SMs
     seg, seg_times = autotune.choose_segment(make_pool, admit_all, candidates=(16, 25, 28, 32), steps=6)
     seg = bcast_int(seg, ws)  # every rank runs rank 0's tiling
+    tuning.update({"segment_rows": seg, "final_segment_rows": 16, "segment_ms": seg_times})
     pool = make_pool(seg)
     admit_all(pool)
     pool.step(args.warmup)
     pool.sync()
     barrier(ws)
     with Clocks(lrank) as clk:
-        ms = pool.step_timed(args.steps)
-    pool.sync()
-    ms = allreduce_max(ms, ws)
-    barrier(ws)
+        blocks = timed_blocks(pool, args.steps, ws)
+    ms = statistics.median(blocks)
     value = ws * B * n * args.steps / (ms / 1e3)
     kernels = pool.kernels_per_step()
     # dominant kernel: Lanczos pass (j = 2), timed alone with CUDA events
@@ -410,12 +508,6 @@ def run_ours(args, ws, rank, lrank):
     peak, peak_kind = hbm_peak()
     pass_bytes = pass_bytes_per_gp() * pts
     achieved = pass_bytes / (pass_ms / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "ncu_lanczos_pass_kg2d.md")
-    if os.path.exists(tpath):
-        for line in open(tpath):
-            if line.startswith("traffic_bytes_per_point:"):
-                traffic = float(line.split(":")[1]) * pts
     step_bytes = step_bytes_per_gp(k) * B * n
     pool.close()
 
@@ -451,39 +543,51 @@ def run_ours(args, ws, rank, lrank):
            "note": "the configuration's complete job (64 x 300^2, 6000 steps, 50 snapshots) through "
                    "nlsb200.Pool: admit (H2D of every input from page-locked memory), 5999 steps, "
                    "every snapshot's D2H into page-locked memory, release; bytes amortised per step"}
-    del outs
+    traj0, vel0 = np.array(outs[0].traj), np.array(outs[0].vel)
+    del outs, pinned
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded kink/Gaussian u0, m = 1 + 0.2 GRF(k^-3))",
-        "config": {"workload": "KG 2-D Gautschi batch, 64 x 300^2 on [-15,15]^2, dt=0.005, nt=6000, ns=50",
-                   "global_batch": B * ws, "per_gpu_batch": B, "grid": [CFG["n"], CFG["n"]],
-                   "k": k, "k_autotune_err": kreport, "segment_rows": seg, "final_segment_rows": 16,
-                   "segment_ms": seg_times, "parallelism": f"trajectory shards x{ws}",
-                   "l2": "working set 0.6 GB per GPU >> 126 MB L2 (no flush needed)"},
+        "config": workload_config(k, ws, B),
+        "timed_blocks": {"blocks": len(blocks), "steps_per_block": args.steps,
+                         "median_ms": ms, "min_ms": min(blocks), "max_ms": max(blocks),
+                         "total_s": sum(blocks) / 1e3},
+        "tuning": tuning,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k2_lanczos1_f32c (2-D FP32 Lanczos pass j=2)",
+                     "frac": achieved / peak, "traffic": TRAFFIC_BYTES_PER_POINT_PASS * pts,
+                     "peak_kind": peak_kind, "kernel": "k2_lanczos1_f32c (2-D FP32 Lanczos pass j=2)",
                      "bytes_per_launch": pass_bytes, "launch_ms": pass_ms},
         "step_roofline": {"algorithmic_bytes_per_gp_step": step_bytes_per_gp(k),
-                          "achieved_GBps": step_bytes * args.steps / (ms / 1e3) / 1e9 * 1.0,
+                          "achieved_GBps": step_bytes * args.steps / (ms / 1e3) / 1e9,
                           "frac": step_bytes * args.steps / (ms / 1e3) / 1e9 / peak},
         "e2e": e2e,
-        "gpu_launches": kernels * args.steps,
+        "gpu_launches": kernels * args.steps * len(blocks),
         "kernels_per_step": kernels,
         "clocks": clk.summary(),
     }
     if ws == 1 and not args.no_serve:
         line["serving"] = serving_leg()
     if ws == 1 and rank == 0 and not args.no_cpu:
-        rate, steps, secs, cores = cpu_oracle_rate(cases)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": f"1 trajectory 300^2, {steps} steps in {secs:.1f} s (FP64 oracle, CGS re-orthogonalisation)"}
+        line["cpu_baseline"], line["parity"] = cpu_parity_leg(k, traj0, vel0)
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def spawn_ranks(n):
+    """--gpus N without a launcher: start the N ranks through
+    torch.distributed.run on 127.0.0.1 with this command line and return
+    their exit status (rank 0 prints the line)."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -492,7 +596,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline and parity leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-mix leg")
     ap.add_argument("--small", action="store_true",
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
@@ -505,7 +609,19 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus < 1:
+        print(f"bench.py: --gpus must be at least 1 (got {args.gpus})", file=sys.stderr)
+        return 2
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args.gpus)
     ws, rank, lrank = dist_init()
+    if ws != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but {ws} rank(s) joined (WORLD_SIZE={ws}); "
+              "launch one process per GPU", file=sys.stderr)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 2
     try:
         if args.impl == "reference":
             return run_reference(args, ws, rank)
