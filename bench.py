@@ -399,14 +399,14 @@ def serving_leg(count=24, rate_hz=8.0, steps=(200, 600), seed=5):
 
 
 def run_small(args, lrank):
-    """--small: --batch trajectories (default 16) of the same workload (k=10,
-    32-row segments), warmup + steps only; the case the ncu captures profile
+    """--small: --batch trajectories (default 16) of the same workload (--k,
+    default the benchmark's; --seg-row segments), warmup + steps only; the case the ncu captures profile
     (16: ~0.2 GB, 64: ~0.7 GB on the GPU, both above the 126 MB L2)."""
     import nlsb200 as nl
     from nlsb200 import workloads as W
     from nlsb200.solver import FP32, KG_GAUTSCHI, Pool
     nl.lib().nls_set_device(lrank)
-    B, k = args.batch, 10
+    B, k = args.batch, args.k
     dim = 3 if args.dim3 else 2
     method = KG_GAUTSCHI
     if args.nlse:
@@ -603,6 +603,7 @@ def main():
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")
     ap.add_argument("--seg", type=int, default=32, help="segment rows (planes in 3-D) of the --small case")
     ap.add_argument("--fseg", type=int, default=0, help="2-D final-pass segment rows of the --small case (0: --seg)")
+    ap.add_argument("--k", type=int, default=K_HEADLINE, help="Krylov dimension of the KG --small case")
     ap.add_argument("--nlse", action="store_true", help="--small case as NLSE 2-D SS2 boxes of 200^2 (k = 12)")
     ap.add_argument("--dim3", type=int, default=0,
                     help="--small case as KG 3-D boxes of DIM3^3 points (0: the 2-D 300^2 workload)")

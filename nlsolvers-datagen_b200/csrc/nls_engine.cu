@@ -139,53 +139,11 @@ cudaError_t launch2_lanczos1(const StepArgs &a, int tiles, cudaStream_t st) {
   k2_lanczos1<E, HC><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
   return cudaGetLastError();
 }
-// Blocks per SM the packed FP32 pass is compiled for (register cap 128 or 168);
-// NLS_F32_BLOCKS=3 selects the 168-register build.
-int f32_minb() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_F32_BLOCKS");
-    return (e && std::atoi(e) == 3) ? 3 : 4;
-  }();
-  return v;
-}
-cudaError_t launch2_lanczos1_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  if (f32_minb() == 3)
-    k2_lanczos1_f32<3><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  else
-    k2_lanczos1_f32<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
-}
-// Packed FP32 pass form: 3 (default) per-warp cp.async shared-memory row ring;
-// 2 register rings with the interior fast path and FP64 dot flushes; 1 the
-// first form (per-row Kahan, row masks everywhere). NLS_F32_PASS selects.
-int f32_pass_form() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_F32_PASS");
-    const int f = e ? std::atoi(e) : 3;
-    return (f == 1 || f == 2) ? f : 3;
-  }();
-  return v;
-}
 cudaError_t launch2_lanczos1_f32c(const StepArgs &a, int tiles, cudaStream_t st) {
-  static const int minb = [] {
-    const char *e = std::getenv("NLS_F32C_BLOCKS");
-    return (e && std::atoi(e) == 5) ? 5 : 4;
-  }();
-  if (minb == 5) return pdl_launch(k2_lanczos1_f32c<5>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
   return pdl_launch(k2_lanczos1_f32c<4>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
-// Packed complex64 pass (NLSE, c == 1); NLS_C32=0 selects the generic
-// one-sequence complex pass, NLS_C32=3 the build for three blocks per SM.
-int c32_mode() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_C32");
-    const int m = e ? std::atoi(e) : 4;
-    return (m == 0 || m == 3) ? m : 4;
-  }();
-  return v;
-}
+// Packed complex64 pass (NLSE, c == 1).
 cudaError_t launch2_lanczos1_c32(const StepArgs &a, int tiles, cudaStream_t st) {
-  if (c32_mode() == 3) return pdl_launch(k2_lanczos1_c32<3>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
   return pdl_launch(k2_lanczos1_c32<4>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
 cudaError_t launch2_first_c32(const StepArgs &a, int tiles, cudaStream_t st) {
@@ -194,40 +152,9 @@ cudaError_t launch2_first_c32(const StepArgs &a, int tiles, cudaStream_t st) {
 cudaError_t launch2_lanczos1_f32c_lo(const StepArgs &a, int tiles, cudaStream_t st) {
   return pdl_launch(k2_lanczos1_f32c<4, true>, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
 }
-cudaError_t launch2_lanczos1_f32b(const StepArgs &a, int tiles, cudaStream_t st) {
-  if (f32_minb() == 3)
-    k2_lanczos1_f32b<3><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  else
-    k2_lanczos1_f32b<4><<<(tiles + WPB - 1) / WPB, 32 * WPB, 0, st>>>(a);
-  return cudaGetLastError();
-}
-// Packed FP32 first pass (one warp per strip and sequence); NLS_F32_FIRST=0
-// selects the generic two-sequence kernel.
-bool f32_first_packed() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_F32_FIRST");
-    return (e && std::atoi(e) == 0) ? 0 : 1;
-  }();
-  return v != 0;
-}
+// Packed FP32 first pass (one warp per strip and sequence).
 cudaError_t launch2_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   return pdl_launch(k2_first_f32, (tiles + WPB - 1) / WPB, 32 * WPB, st, a);
-}
-cudaError_t launch2t_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k2t_lanczos_f32<<<tiles, 128, sizeof(TmaSmem), st>>>(a);
-  return cudaGetLastError();
-}
-cudaError_t attrs_tma_f32() {
-  return set_smem(k2t_lanczos_f32, sizeof(TmaSmem));
-}
-// NLS_TMA=1 selects the TMA-pipelined FP32 pass; the register-ring pass is the
-// default (it issues half the instructions and needs no per-row barrier).
-bool use_tma() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_TMA");
-    return (e && std::atoi(e) == 1) ? 1 : 0;
-  }();
-  return v != 0;
 }
 template <typename E, int NSEQ, int FIN, bool HC>
 cudaError_t launch2_final(const StepArgs &a, int tiles, cudaStream_t st) {
@@ -239,15 +166,8 @@ cudaError_t launch2_sv(const StepArgs &a, int tiles, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// 3-D FP32 warp-marching pass (one block per strip, band, segment and
-// sequence of the block table); NLS_K3=0 selects the shared-memory plane kernel.
-bool use_k3() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_K3");
-    return (e && std::atoi(e) == 0) ? 0 : 1;
-  }();
-  return v != 0;
-}
+// 3-D FP32 warp-marching passes (one block per strip, band, segment and
+// sequence of the block table).
 cudaError_t launch3_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   k3_first_f32<<<tiles, 32 * BY3, 0, st>>>(a);
   return cudaGetLastError();
@@ -280,19 +200,11 @@ template <int DIM, typename R> cudaError_t launch_sv(const StepArgs &a, int grid
   k_sv<DIM, R><<<grid, dim3(Geo<DIM>::TX, Geo<DIM>::TY), smem_sv<DIM, R>(), st>>>(a);
   return cudaGetLastError();
 }
-// f(T): the register-resident kernel for k <= 16, the shared-memory one above
-// (NLS_FTRI=smem forces the latter).
-bool ftri_smem_only() {
-  static int v = [] {
-    const char *e = std::getenv("NLS_FTRI");
-    return (e && std::strcmp(e, "smem") == 0) ? 1 : 0;
-  }();
-  return v != 0;
-}
+// f(T): the register-resident kernel for k <= 16, the shared-memory one above.
 template <typename E> cudaError_t launch_ftri(const StepArgs &a, int nslots_cap, cudaStream_t st) {
   const int warps = nslots_cap * a.nseq;
   const int blocks = (warps + 3) / 4;
-  if (ftri_smem_only() || a.k > 16) return pdl_launch(k_ftri<E>, blocks, 128, st, a);
+  if (a.k > 16) return pdl_launch(k_ftri<E>, blocks, 128, st, a);
   if (a.k <= 8) return pdl_launch(k_ftri_reg<E, 8>, blocks, 128, st, a);
   if (a.k <= 12) return pdl_launch(k_ftri_reg<E, 12>, blocks, 128, st, a);
   return pdl_launch(k_ftri_reg<E, 16>, blocks, 128, st, a);
@@ -309,7 +221,6 @@ cudaError_t launch_advance(const StepArgs &a, int nslots_cap, cudaStream_t st) {
 struct KSet {
   Launch kg, ss2, sewi_a, sewi_b;  // Gautschi / NLSE phases
   LaunchFn sv[2] = {nullptr, nullptr};
-  LaunchFn lanczos_tma = nullptr;  // 2-D FP32 c == 1 TMA-pipelined pass (tile table `tt`)
   cudaError_t (*ftri)(const StepArgs &, int, cudaStream_t) = nullptr;
   cudaError_t (*ring)(const StepArgs &, int, int, cudaStream_t) = nullptr;
   cudaError_t (*set_attrs)() = nullptr;
@@ -347,14 +258,12 @@ template <typename R> KSet make_real3() {
   k.kg.lanczos[0] = k.kg.lanczos[1] = launch_lanczos<3, R, 2>;
   k.kg.final_[0] = k.kg.final_[1] = launch_final<3, R, 2, FIN_KG>;
   if constexpr (sizeof(R) == 4) {
-    if (use_k3()) {
-      k.kg.first[0] = launch3_first_f32;
-      k.kg.first_tt[0] = true;
-      k.kg.lanczos[0] = launch3_lanczos_f32;
-      k.kg.lanczos_tt[0] = true;
-      k.kg.final_[0] = launch3_final_f32;
-      k.kg.final_tt[0] = true;
-    }
+    k.kg.first[0] = launch3_first_f32;
+    k.kg.first_tt[0] = true;
+    k.kg.lanczos[0] = launch3_lanczos_f32;
+    k.kg.lanczos_tt[0] = true;
+    k.kg.final_[0] = launch3_final_f32;
+    k.kg.final_tt[0] = true;
   }
   k.sv[0] = k.sv[1] = launch_sv<3, R>;
   k.ftri = launch_ftri<R>;
@@ -386,16 +295,10 @@ template <typename R> KSet make_real2() {
   k.kg.lanczos[0] = launch2_lanczos1<R, false>;
   k.kg.lanczos[1] = launch2_lanczos1<R, true>;
   if constexpr (sizeof(R) == 4) {
-    k.kg.lanczos[0] = f32_pass_form() == 1   ? launch2_lanczos1_f32
-                      : f32_pass_form() == 3 ? launch2_lanczos1_f32c
-                                             : launch2_lanczos1_f32b;  // packed FP32x2
-    if (f32_first_packed()) {
-      k.kg.first[0] = launch2_first_f32;
-      k.kg.first_lt[0] = true;
-    }
-    if (f32_pass_form() == 3) k.kg.lanczos_lo[0] = launch2_lanczos1_f32c_lo;
-    k.lanczos_tma = launch2t_lanczos_f32;
-    k.set_attrs = attrs_tma_f32;
+    k.kg.lanczos[0] = launch2_lanczos1_f32c;  // packed FP32x2, per-warp cp.async row rings
+    k.kg.first[0] = launch2_first_f32;
+    k.kg.first_lt[0] = true;
+    k.kg.lanczos_lo[0] = launch2_lanczos1_f32c_lo;
   }
   k.kg.final_[0] = launch2_final<R, 2, FIN_KG, false>;
   k.kg.final_[1] = launch2_final<R, 2, FIN_KG, true>;
@@ -403,7 +306,7 @@ template <typename R> KSet make_real2() {
   k.sv[1] = launch2_sv<R, true>;
   k.ftri = launch_ftri<R>;
   k.ring = launch_ring<R, 0>;
-  if (!k.set_attrs) k.set_attrs = attrs_none;
+  k.set_attrs = attrs_none;
   return k;
 }
 template <typename E> KSet make_cplx2() {
@@ -427,11 +330,9 @@ template <typename E> KSet make_cplx2() {
   k.sewi_b.final_[0] = launch2_final<E, 1, FIN_SEWI_B, false>;
   k.sewi_b.final_[1] = launch2_final<E, 1, FIN_SEWI_B, true>;
   if constexpr (std::is_same<E, Cx<float>>::value) {
-    if (c32_mode() != 0) {
-      k.ss2.lanczos[0] = k.sewi_a.lanczos[0] = k.sewi_b.lanczos[0] = launch2_lanczos1_c32;
-      k.ss2.first[0] = launch2_first_c32;
-      k.ss2.first_lt[0] = true;
-    }
+    k.ss2.lanczos[0] = k.sewi_a.lanczos[0] = k.sewi_b.lanczos[0] = launch2_lanczos1_c32;
+    k.ss2.first[0] = launch2_first_c32;
+    k.ss2.first_lt[0] = true;
   }
   k.ftri = launch_ftri<E>;
   k.ring = launch_ring<E, 1>;
@@ -919,28 +820,19 @@ StepArgs base_args(const nls_pool *P, const TileSet &T, int group = 0) {
   // the packed FP32 Gautschi forms read the cosine start vector from u_hi
   // (2-D and 3-D, c == 1)
   const bool fam = P->prec == NLS_FP32 && !P->cplx && !P->step_hc && !is_sv(P->method);
-  a.v0_u = fam && ((P->dim == 2 && f32_first_packed() && f32_pass_form() == 3 && !use_tma()) ||
-                   (P->dim == 3 && use_k3()))
-               ? 1
-               : 0;
+  a.v0_u = fam ? 1 : 0;
   return a;
 }
 
 // Tile table, tile count and grid of the Lanczos passes j >= 1 of family L:
-// 2-D passes run one warp per (strip, sequence) of `lt` (or one TMA block per
-// tile of `tt`), 3-D FP32 passes one block per tile of `tt`, the other 3-D
-// passes one block per tile of `tiles` with both sequences.
+// 2-D passes run one warp per (strip, sequence) of `lt`, 3-D FP32 passes one
+// block per tile of `tt`, the other 3-D passes one block per tile of `tiles`
+// with both sequences.
 LaunchFn pass_args(const nls_pool *P, const TileSet &T, const Launch &L, StepArgs &b, int &grid) {
   const int hc = P->step_hc;
   grid = T.cap;
   LaunchFn lf = L.lanczos[hc];
-  if (P->dim == 2 && hc == 0 && P->ks.lanczos_tma && &L == &P->ks.kg && use_tma()) {
-    b.tiles = T.d_tt;
-    b.ntiles = b.nseq == 2 ? T.d_ntt2 : T.d_ntt1;
-    b.lt_stride = T.d_ntt1;
-    grid = T.tcap;
-    lf = P->ks.lanczos_tma;
-  } else if (P->dim == 2) {
+  if (P->dim == 2) {
     b.tiles = T.d_lt;
     b.ntiles = b.nseq == 2 ? T.d_nlt2 : T.d_nlt1;
     b.lt_stride = T.d_nlt1;

@@ -1332,165 +1332,11 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32(StepArgs a) {
   }
 }
 
-// Second form of the packed FP32 pass, with less work per row:
-//  - segments whose rows r0-2 .. r1+1 are interior rows of the grid (r0 >= 2,
-//    r1 <= ny-2) run a march without row predicates or row masks (EDGE false);
-//    the first and last segment of each trajectory keep them (EDGE true);
-//  - the column mask of v_j and z is folded into the per-lane coefficients
-//    (V rows outside the grid columns are zero, so only the stencil term needs it);
-//  - dot products: FP32 pair sums over three rows, added into FP64 accumulators;
-//    the scale of V_{j-1} (1/beta0 at j = 1) is applied to the finished sums;
-//  - rows are prefetched only up to the last row the segment needs.
-template <bool EDGE>
-__device__ __forceinline__ void lz1f32_march(const float *pA, const float *pB, float *pJ, int P, int r0, int r1,
-                                             int ny, bool ld, bool io, bool hasB, float2 CA, float2 CB,
-                                             const F4 &CSx, const F4 &OPx, const F4 &xmiss, double *acc) {
-  const F4 zero4 = F4{f2(0.f), f2(0.f)};
-  auto rowA = [&](int r) -> F4 {
-    const bool ok = EDGE ? (ld && r >= 0 && r < ny && r <= r1 + 1) : (ld && r <= r1 + 1);
-    return ok ? f4_load(pA + r * P) : zero4;
-  };
-  auto rowB = [&](int r) -> F4 {
-    const bool ok = EDGE ? (ld && hasB && r >= 0 && r < ny && r <= r1) : (ld && hasB && r <= r1);
-    return ok ? f4_load(pB + r * P) : zero4;
-  };
-  float2 q0 = f2(0.f), q1 = f2(0.f), q2 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f), q5 = f2(0.f);
-  F4 A0 = rowA(r0 - 2), A1 = rowA(r0 - 1), A2 = rowA(r0), A3 = rowA(r0 + 1), A4 = rowA(r0 + 2),
-     A5 = rowA(r0 + 3);
-  F4 B0 = rowB(r0 - 1), B1 = rowB(r0), B2 = rowB(r0 + 1);
-  F4 V0 = zero4, V1 = zero4, V2 = zero4;
-  const int qb = r0 - 1;
-  const int nit = ((r1 - qb + 1) + 5) / 6 * 6;
-#define NLSB_ROW2(Am, Ac, Ap, Af, Bc, Vm, Vc, Vn, FLUSH)                                        \
-  {                                                                                           \
-    const int q = qb + it;                                                                    \
-    {                                                                                         \
-      const float lft = __shfl_up_sync(0xffffffffu, Ac.b.y, 1);                               \
-      const float rgt = __shfl_down_sync(0xffffffffu, Ac.a.x, 1);                             \
-      F4 miss = xmiss;                                                                        \
-      if (EDGE) {                                                                             \
-        const float2 rm = f2(float((q == 0) + (q == ny - 1)));                                \
-        miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                      \
-      }                                                                                       \
-      const F4 w = lap4(Am, Ac, Ap, lft, rgt, miss);                                          \
-      Vn.a = fma2(CB, Bc.a, fma2(CA, Ac.a, mul2(CSx.a, w.a)));                                \
-      Vn.b = fma2(CB, Bc.b, fma2(CA, Ac.b, mul2(CSx.b, w.b)));                                \
-      if (EDGE) {                                                                             \
-        const float2 rv = f2((q >= 0 && q < ny) ? 1.f : 0.f);                                 \
-        Vn.a = mul2(Vn.a, rv);                                                                \
-        Vn.b = mul2(Vn.b, rv);                                                                \
-      }                                                                                       \
-      if (io && q >= r0 && q < r1) f4_store(pJ + q * P, Vn);                                  \
-    }                                                                                         \
-    {                                                                                         \
-      const int r = q - 1;                                                                    \
-      const float lft = __shfl_up_sync(0xffffffffu, Vc.b.y, 1);                               \
-      const float rgt = __shfl_down_sync(0xffffffffu, Vc.a.x, 1);                             \
-      if (r >= r0 && r < r1) {                                                                \
-        F4 miss = xmiss;                                                                      \
-        if (EDGE) {                                                                           \
-          const float2 rm = f2(float((r == 0) + (r == ny - 1)));                              \
-          miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};                                    \
-        }                                                                                     \
-        F4 z = lap4(Vm, Vc, Vn, lft, rgt, miss);                                              \
-        z.a = mul2(z.a, OPx.a);                                                               \
-        z.b = mul2(z.b, OPx.b);                                                               \
-        q0 = fma2(z.a, Am.a, fma2(z.b, Am.b, q0));                                            \
-        q1 = fma2(z.a, Vc.a, fma2(z.b, Vc.b, q1));                                            \
-        q2 = fma2(Am.a, Vc.a, fma2(Am.b, Vc.b, q2));                                          \
-        q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));                                              \
-        q4 = fma2(Vc.a, Vc.a, fma2(Vc.b, Vc.b, q4));                                          \
-        q5 = fma2(Am.a, Am.a, fma2(Am.b, Am.b, q5));                                          \
-      }                                                                                       \
-    }                                                                                         \
-    if (FLUSH) {                                                                              \
-      acc[0] += (double)(q0.x + q0.y);                                                        \
-      acc[1] += (double)(q1.x + q1.y);                                                        \
-      acc[2] += (double)(q2.x + q2.y);                                                        \
-      acc[3] += (double)(q3.x + q3.y);                                                        \
-      acc[4] += (double)(q4.x + q4.y);                                                        \
-      acc[5] += (double)(q5.x + q5.y);                                                        \
-      q0 = q1 = q2 = q3 = q4 = q5 = f2(0.f);                                                  \
-    }                                                                                         \
-    Af = rowA(q + 5);                                                                         \
-    Bc = rowB(q + 3);                                                                         \
-  }
-  for (int it0 = 0; it0 < nit; it0 += 6) {
-    int it = it0;
-    NLSB_ROW2(A0, A1, A2, A0, B0, V1, V2, V0, false) ++it;
-    NLSB_ROW2(A1, A2, A3, A1, B1, V2, V0, V1, false) ++it;
-    NLSB_ROW2(A2, A3, A4, A2, B2, V0, V1, V2, true) ++it;
-    NLSB_ROW2(A3, A4, A5, A3, B0, V1, V2, V0, false) ++it;
-    NLSB_ROW2(A4, A5, A0, A4, B1, V2, V0, V1, false) ++it;
-    NLSB_ROW2(A5, A0, A1, A5, B2, V0, V1, V2, true)
-  }
-#undef NLSB_ROW2
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32b(StepArgs a) {
-  using E = float;
-  WARP_TILE_PROLOGUE
-  const int j = a.j, sq = t.local & 1;
-  const float opsc = float(a.op_sign * s.inv_h2);
-  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
-  const double b0 = a.beta0[t.slot * 2 + sq];
-  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
-  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
-  const float cs = float(sA * L.inv_b) * opsc;
-  const float2 CA = f2(float(-L.ar * sA * L.inv_b)), CB = f2(float(-L.dr * sB * L.inv_b));
-  const long long vo = (long long)sq * a.kv;
-  const bool hasB = j >= 2;
-  const long long lane_off = s.off + S.col0;
-  const float *pA = (const float *)a.V + (vo + j - 1) * a.vstride + lane_off;
-  const float *pB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
-  float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
-  // per-element column masks folded into the stencil coefficients, and the
-  // missing-neighbour counts of the x direction
-  F4 CSx, OPx, xmiss;
-  {
-    float v[4], m[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int x = S.col0 + e;
-      v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
-      m[e] = float((x == 0) + (x == S.nx - 1));
-    }
-    CSx = F4{make_float2(v[0] * cs, v[1] * cs), make_float2(v[2] * cs, v[3] * cs)};
-    OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
-    xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
-  }
-  const bool ld = S.lane_in, io = S.out_lane;
-  const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  if (r0 >= 2 && r1 <= ny - 2)
-    lz1f32_march<false>(pA, pB, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc);
-  else
-    lz1f32_march<true>(pA, pB, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc);
-  // the stored V_{j-1} is s0 v_{j-1} at j = 1 (V_0 holds the raw start vector)
-  acc[0] *= sA;
-  acc[2] *= sA;
-  acc[5] *= sA * sA;
-  constexpr int ND = 6;
-  double vals[ND];
-#pragma unroll
-  for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
-  const int tc = s.tile_count, TT = *a.lt_stride;
-  if (warp_publish<ND>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot * 2 + sq,
-                       tc, lane)) {
-    const double *part = a.part + (long long)j * a.part_stride;
-    const double tot = warp_slot_total<ND>(part, sq * TT + s.tile_begin, tc, lane);
-    double tv[ND];
-#pragma unroll
-    for (int q = 0; q < ND; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
-    if (lane == 0) {
-      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
-      a.ticket[t.slot * 2 + sq] = 0;
-    }
-  }
-}
-
-// Third form of the packed FP32 pass: the rows of V_{j-1} and V_{j-2} are
+// Default form of the packed FP32 pass (k2_lanczos1_f32c): segments whose rows
+// r0-2 .. r1+1 are interior rows of the grid run a march without row
+// predicates or row masks; the column masks are folded into the per-lane
+// coefficients; dot products are FP32 pair sums over three rows, added into
+// FP64 accumulators. The rows of V_{j-1} and V_{j-2} are
 // streamed by each lane's own 16-byte cp.async copies into a per-warp
 // shared-memory ring CPD rows ahead. Rows in flight cost no registers and no
 // barrier is needed (a lane reads back only the cells it copied; x-neighbours
@@ -1872,286 +1718,6 @@ static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
       double b0;
       a.scal[(t.slot * 2 + sq) * KMAX + 0] = lz_first<false>(tv, Eps<float>::v, b0);
       a.beta0[t.slot * 2 + sq] = b0;
-      a.ticket[t.slot * 2 + sq] = 0;
-    }
-  }
-}
-
-// ---------------------- TMA-pipelined FP32 Lanczos pass (2-D, c == 1)
-// One block (4 warps) per (slot, sequence, column tile of <= 512 columns, row
-// segment). Thread 0 streams the rows of V_{j-1} and V_{j-2} with 1-D bulk
-// copies (cp.async.bulk, completion counted on an mbarrier per ring slot)
-// TD rows ahead into shared-memory rings; rows outside the grid are copied
-// from a device buffer of zeros. Thread t owns columns x0+4t .. x0+4t+3; the
-// new v_j row goes through a 3-slot shared ring so that the z-stencil reads
-// its x-neighbours after one block barrier per row. Waits on the mbarriers are
-// bounded: on expiry the block records NLS_ERR status 3 in the slot and stops.
-namespace tma {
-constexpr int TD = 10;        // rows in flight ahead
-constexpr int RA = TD + 3;    // V_{j-1} ring
-constexpr int RB = TD + 1;    // V_{j-2} ring
-constexpr int TW = 512;       // max tile width (columns)
-constexpr int RW = TW + 8;    // row slot: 4 halo + TW + 4 halo
-constexpr unsigned SPIN_LIMIT = 1u << 26;
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *m, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *m) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(m))
-      : "memory");
-}
-// true when the phase with the given parity has completed; bounded spin
-__device__ __forceinline__ bool mbar_wait(uint64_t *m, unsigned parity) {
-  const unsigned a = smem_u32(m);
-  for (unsigned it = 0; it < SPIN_LIMIT; ++it) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-}  // namespace tma
-
-struct TmaSmem {
-  float A[tma::RA][tma::RW];
-  float B[tma::RB][tma::RW];
-  float V[3][tma::RW];
-  uint64_t barA[tma::RA];
-  uint64_t barB[tma::RB];
-  double red[4][8];
-  int last;
-};
-
-static __global__ void __launch_bounds__(128, 3) k2t_lanczos_f32(StepArgs a) {
-  extern __shared__ __align__(128) unsigned char tma_raw[];
-  TmaSmem &M = *reinterpret_cast<TmaSmem *>(tma_raw);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if ((int)blockIdx.x >= *a.ntiles) return;
-  const TileDesc t = a.tiles[blockIdx.x];
-  const SlotDesc &s = a.slots[t.slot];
-  const int j = a.j, sq = t.local & 1;
-  const int x0 = t.x0, Wc = t.y0, r0 = t.p0, r1 = t.p1, nx = s.nx, ny = s.ny;
-  const long long P = s.pitch;
-  const float opsc = float(a.op_sign * s.inv_h2);
-  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
-  const double b0 = a.beta0[t.slot * 2 + sq];
-  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
-  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
-  const float2 CS = f2(float(sA * L.inv_b) * opsc), CA = f2(float(-L.ar * sA * L.inv_b)),
-               CB = f2(float(-L.dr * sB * L.inv_b)), SA = f2(float(sA)), OP = f2(opsc);
-  const bool hasB = j >= 2;
-  const long long vo = (long long)sq * a.kv;
-  const float *gA = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
-  const float *gB = (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + s.off;
-  float *gJ = (float *)a.V + (vo + j) * a.vstride + s.off;
-  const float *zeros = (const float *)a.zeros;
-  // copy window of a row: columns [cb, ce) land at slot offset (cb - (x0 - 4))
-  const int cb = max(x0 - 4, 0), ce = min(x0 + Wc + 4, (int)P);
-  const unsigned cbytes = (unsigned)(ce - cb) * 4u;
-  const int soff = cb - (x0 - 4);
-  // zero every slot once (halo columns outside [cb, ce) stay zero), init barriers
-  for (int i = tid; i < (tma::RA + tma::RB + 3) * tma::RW; i += blockDim.x) (&M.A[0][0])[i] = 0.f;
-  if (tid == 0) {
-    for (int q = 0; q < tma::RA; ++q) tma::mbar_init(&M.barA[q], 1);
-    for (int q = 0; q < tma::RB; ++q) tma::mbar_init(&M.barB[q], 1);
-    tma::fence_mbar_init();
-  }
-  tma::fence_async_smem();
-  __syncthreads();
-  // row streams: A rows r0-2 .. r1+1 (sequence number ia = row - (r0-2)),
-  // B rows r0-1 .. r1 (ib = row - (r0-1))
-  const int nA = (r1 + 1) - (r0 - 2) + 1, nB = hasB ? (r1 - (r0 - 1) + 1) : 0;
-  auto issueA = [&](int ia) {
-    if (ia >= nA) return;
-    const int row = r0 - 2 + ia, sl = ia % tma::RA;
-    const float *src = (row >= 0 && row < ny) ? gA + row * P + cb : zeros;
-    tma::mbar_expect_tx(&M.barA[sl], cbytes);
-    tma::bulk_g2s(&M.A[sl][soff], src, cbytes, &M.barA[sl]);
-  };
-  auto issueB = [&](int ib) {
-    if (ib >= nB) return;
-    const int row = r0 - 1 + ib, sl = ib % tma::RB;
-    const float *src = (row >= 0 && row < ny) ? gB + row * P + cb : zeros;
-    tma::mbar_expect_tx(&M.barB[sl], cbytes);
-    tma::bulk_g2s(&M.B[sl][soff], src, cbytes, &M.barB[sl]);
-  };
-  int issuedA = 0, issuedB = 0;  // meaningful in thread 0
-  if (tid == 0) {
-    for (int i = 0; i < tma::TD + 2; ++i) issueA(i);
-    for (int i = 0; i < tma::TD; ++i) issueB(i);
-    issuedA = min(tma::TD + 2, nA);
-    issuedB = min(tma::TD, nB);
-  }
-  // thread columns
-  const int c4 = 4 * tid;
-  const bool act = c4 < Wc;
-  const int gx = x0 + c4;
-  F4 xval, xmiss;
-  {
-    float v[4], m[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int x = gx + e;
-      v[e] = (act && x < nx) ? 1.f : 0.f;
-      m[e] = float((x == 0) + (x == nx - 1));
-    }
-    xval = F4{make_float2(v[0], v[1]), make_float2(v[2], v[3])};
-    xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
-  }
-  const int sc = 4 + c4;  // column of element 0 inside a slot
-  auto lds4 = [&](const float *row) -> F4 {
-    const float4 v = *reinterpret_cast<const float4 *>(row + sc);
-    return F4{make_float2(v.x, v.y), make_float2(v.z, v.w)};
-  };
-  // v_j at a single column xc (slot column cs) of row q: the halo columns of a
-  // tile that does not span the row are formed by the edge threads
-  auto v_single = [&](const float *Am, const float *Ac, const float *Ap, const float *Bq, int csl,
-                      int xc, int q) -> float {
-    if (!(xc >= 0 && xc < nx && q >= 0 && q < ny)) return 0.f;
-    const float c = Ac[csl];
-    float acc = ((Ac[csl - 1] - c) + (Ac[csl + 1] - c)) + ((Am[csl] - c) + (Ap[csl] - c));
-    acc = fmaf(float((xc == 0) + (xc == nx - 1) + (q == 0) + (q == ny - 1)), c, acc);
-    float v = CS.x * acc + CA.x * c;
-    if (Bq) v = fmaf(CB.x, Bq[csl], v);
-    return v;
-  };
-  const bool left_halo = x0 > 0, right_halo = x0 + Wc < nx;
-  const int last_t = (Wc + 3) / 4 - 1;
-  Kahan<float> k0, k1, k2, k3, k4, k5;
-  k0.init(); k1.init(); k2.init(); k3.init(); k4.init(); k5.init();
-  bool ok = true;
-  const F4 z4 = F4{f2(0.f), f2(0.f)};
-  F4 vm2 = z4, vm1 = z4;  // own v rows q-2, q-1
-  int waitedA = 0, waitedB = 0;
-  // A rows r0-2 and r0-1 are read in the first step besides r0
-  ok = tma::mbar_wait(&M.barA[0], 0u);
-  if (ok) waitedA = 1;
-  ok = ok && tma::mbar_wait(&M.barA[1], 0u);
-  if (ok) waitedA = 2;
-  // steps q = r0-1 .. r1: v(q), then z(q-1)
-  for (int q = r0 - 1; q <= r1; ++q) {
-    const int ia = q + 1 - (r0 - 2);  // A row q+1
-    const int ib = q - (r0 - 1);      // B row q
-    if (ok) {
-      const bool okA = tma::mbar_wait(&M.barA[ia % tma::RA], (unsigned)((ia / tma::RA) & 1));
-      if (okA) waitedA = ia + 1;
-      bool okB = true;
-      if (hasB) {
-        okB = tma::mbar_wait(&M.barB[ib % tma::RB], (unsigned)((ib / tma::RB) & 1));
-        if (okB) waitedB = ib + 1;
-      }
-      ok = okA && okB;
-    }
-    const float *Am = M.A[(ia - 2) % tma::RA], *Ac = M.A[(ia - 1) % tma::RA], *Ap = M.A[ia % tma::RA];
-    const float *Bq = hasB ? M.B[ib % tma::RB] : nullptr;
-    float *Vs = M.V[(q + 3) % 3];
-    F4 vq = z4, am = z4;
-    if (ok && act) {
-      am = lds4(Am);
-      const F4 ac = lds4(Ac), ap = lds4(Ap);
-      const float lft = Ac[sc - 1], rgt = Ac[sc + 4];
-      const float2 rm = f2(float((q == 0) + (q == ny - 1)));
-      const F4 miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};
-      const F4 w = lap4(am, ac, ap, lft, rgt, miss);
-      const F4 bq = hasB ? lds4(Bq) : z4;
-      const float2 rv = f2((q >= 0 && q < ny) ? 1.f : 0.f);
-      vq.a = mul2(mul2(fma2(CB, bq.a, fma2(CA, ac.a, mul2(CS, w.a))), xval.a), rv);
-      vq.b = mul2(mul2(fma2(CB, bq.b, fma2(CA, ac.b, mul2(CS, w.b))), xval.b), rv);
-      *reinterpret_cast<float4 *>(&Vs[sc]) = make_float4(vq.a.x, vq.a.y, vq.b.x, vq.b.y);
-      if (q >= r0 && q < r1) f4_store(gJ + q * P + gx, vq);
-      if (tid == 0 && left_halo) Vs[3] = v_single(Am, Ac, Ap, Bq, 3, x0 - 1, q);
-      if (tid == last_t && right_halo) Vs[4 + Wc] = v_single(Am, Ac, Ap, Bq, 4 + Wc, x0 + Wc, q);
-    }
-    ok = __syncthreads_and(ok) != 0;
-    if (!ok) break;
-    if (tid == 0) {  // ring slots of rows q-2 (A) and q-1 (B) are free now
-      tma::fence_async_smem();
-      issueA(ia + tma::TD);
-      issueB(ib + tma::TD);
-      issuedA = min(ia + tma::TD + 1, nA);
-      issuedB = min(ib + tma::TD + 1, nB);
-    }
-    const int r = q - 1;
-    if (act && r >= r0 && r < r1) {
-      const float *Vr = M.V[(r + 3) % 3];
-      const float lft = Vr[sc - 1], rgt = Vr[sc + 4];
-      const float2 rm = f2(float((r == 0) + (r == ny - 1)));
-      const F4 miss = F4{add2(xmiss.a, rm), add2(xmiss.b, rm)};
-      F4 z = lap4(vm2, vm1, vq, lft, rgt, miss);
-      z.a = mul2(mul2(z.a, OP), xval.a);
-      z.b = mul2(mul2(z.b, OP), xval.b);
-      // v_{j-1}(r) = sA * A(r): A row r = q-1 is the `am` row of this step
-      const F4 vm = F4{mul2(am.a, SA), mul2(am.b, SA)};
-      float2 d0 = fma2(z.a, vm.a, mul2(z.b, vm.b)), d1 = fma2(z.a, vm1.a, mul2(z.b, vm1.b));
-      float2 d2 = fma2(vm.a, vm1.a, mul2(vm.b, vm1.b)), d3 = fma2(z.a, z.a, mul2(z.b, z.b));
-      float2 d4 = fma2(vm1.a, vm1.a, mul2(vm1.b, vm1.b)), d5 = fma2(vm.a, vm.a, mul2(vm.b, vm.b));
-      k0.add(d0.x + d0.y); k1.add(d1.x + d1.y); k2.add(d2.x + d2.y);
-      k3.add(d3.x + d3.y); k4.add(d4.x + d4.y); k5.add(d5.x + d5.y);
-    }
-    vm2 = vm1;
-    vm1 = vq;
-  }
-  if (!ok) {
-    // a bulk copy did not complete within the bound: record the error, then
-    // wait (bounded) for every copy still targeting this block's shared memory
-    if (tid == 0) {
-      a.state[t.slot].status = -10;
-      for (int ia = waitedA; ia < issuedA; ++ia)
-        tma::mbar_wait(&M.barA[ia % tma::RA], (unsigned)((ia / tma::RA) & 1));
-      for (int ib = waitedB; ib < issuedB; ++ib)
-        tma::mbar_wait(&M.barB[ib % tma::RB], (unsigned)((ib / tma::RB) & 1));
-    }
-    __syncthreads();
-    return;
-  }
-  // block reduction of the six dots (FP64), then the slot's last block
-  double v6[6] = {k0.val(), k1.val(), k2.val(), k3.val(), k4.val(), k5.val()};
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    double v = v6[q];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) M.red[warp][q] = v;
-  }
-  __syncthreads();
-  const int tc = s.tile_count2, TT = *a.lt_stride;
-  double *part = a.part + (long long)j * a.part_stride;
-  if (tid == 0) {
-    for (int q = 0; q < 6; ++q)
-      __stcg(part + (long long)blockIdx.x * 6 + q, ((M.red[0][q] + M.red[1][q]) + M.red[2][q]) + M.red[3][q]);
-    __threadfence();
-    M.last = atomicAdd(a.ticket + t.slot * 2 + sq, 1) == tc - 1;
-  }
-  __syncthreads();
-  if (M.last && warp == 0) {
-    __threadfence();
-    const double tot = warp_slot_total<6>(part, sq * TT + s.tile_begin2, tc, lane);
-    double tv[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) tv[q] = __shfl_sync(0xffffffffu, tot, q);
-    if (lane == 0) {
-      a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
       a.ticket[t.slot * 2 + sq] = 0;
     }
   }
