@@ -182,6 +182,25 @@ int nls_pool_set_downsample(nls_pool *pool, int32_t slot, const int32_t *target,
    Computed on the current device (synchronous). */
 int nls_downsample_linear(int32_t dim, const int64_t *shape, const int64_t *target, const double *half_widths,
                           int32_t frames, int32_t is_complex, const double *in, double *out);
+/* Spectral downsampling of every snapshot of the slot on the device before its
+   copy to the host: the reference's downsample_fft / downsample_fft_3d
+   (scripts/downsampling.py:10-35, :147-178), which its 3-D NLSE launcher
+   applies to the snapshots (scripts/complex_launcher_3d.py:185-187). Per array
+   axis the orthonormal DFT is taken, the fftshift-ed spectrum cropped to the
+   centred `target` bins (from (n - t)/2), ifftshift-ed and inverse-transformed
+   (orthonormal); real fields keep the real part. 1 <= target <= source extent
+   on every axis. Outputs, call order and the full-size outputs as
+   nls_pool_set_downsample. FP64; agrees with the reference's torch FFT to
+   about 1e-14 relative. */
+int nls_pool_set_downsample_fft(nls_pool *pool, int32_t slot, const int32_t *target, double *traj_dst,
+                                double *vel_dst);
+/* The same spectral crop on host arrays, a drop-in for downsample_fft(u,
+   target_shape) and downsample_fft_3d(u, target_shape)
+   (scripts/downsampling.py:10-35, :147-178): `frames` C-order arrays of
+   shape[0..dim-1] (complex128 when is_complex) into `frames` arrays of
+   target[0..dim-1]. Computed on the current device (synchronous). */
+int nls_downsample_fft(int32_t dim, const int64_t *shape, const int64_t *target, int32_t frames, int32_t is_complex,
+                       const double *in, double *out);
 /* Free the slot (waits for its outstanding snapshot copies). */
 int nls_pool_release(nls_pool *pool, int32_t slot);
 /* Wait for all queued device work and copies. */

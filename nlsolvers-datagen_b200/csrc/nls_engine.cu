@@ -19,6 +19,7 @@
 #include "../../include/nlsb200.h"
 #include "nls_kernels.cuh"
 #include "nls_downsample.cuh"
+#include "nls_fft_downsample.cuh"
 
 using namespace nlsb;
 
@@ -417,6 +418,8 @@ struct SlotHost {
   double *ds_traj = nullptr, *ds_vel = nullptr;
   bool reg_ds_traj = false, reg_ds_vel = false;
   void *ds_dev = nullptr;                    // tables and staging frame (one allocation)
+  bool ds_fft = false;                       // spectral crop (nls_pool_set_downsample_fft) instead of linear
+  FftDsPlan ds_plan{};                       // its matrices and work buffers (inside ds_dev)
   // completion of each snapshot's copies (snapshot si >= 1), for nls_pool_snapshots_ready
   std::vector<cudaEvent_t> snap_ev;
   int snaps_ready = 1;
@@ -1054,10 +1057,16 @@ int enqueue_diag(nls_pool *P, int s, int si, int f, cudaStream_t st) {
 int enqueue_downsample(nls_pool *P, SlotHost &h, const double *frame, int si, cudaStream_t st) {
   const DsGeom &g = h.ds_geom;
   double *stage = (double *)h.ds_dev;
-  const int64_t total = h.ds_frame;
-  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-  k_downsample<<<blocks, 256, 0, st>>>(g, frame, stage, 1);
-  CK(cudaGetLastError());
+  if (h.ds_fft) {
+    const int real = g.comps == 1 ? 1 : 0;
+    for (int f = 0; f < g.nfields; ++f)
+      CK(fft_ds_field(h.ds_plan, frame + (int64_t)f * g.src_field, real, stage + (int64_t)f * g.dst_field, real, st));
+  } else {
+    const int64_t total = h.ds_frame;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    k_downsample<<<blocks, 256, 0, st>>>(g, frame, stage, 1);
+    CK(cudaGetLastError());
+  }
   CK(cudaMemcpyAsync(h.ds_traj + (int64_t)si * g.dst_field, stage, sizeof(double) * g.dst_field,
                      cudaMemcpyDeviceToHost, st));
   if (g.nfields == 2 && h.ds_vel)
@@ -1615,7 +1624,9 @@ int nls_pool_set_diagnostics(nls_pool *P, int32_t s, double *diag_dst) {
   return enqueue_diag(P, s, 0, 0, P->stream);
 }
 
-int nls_pool_set_downsample(nls_pool *P, int32_t s, const int32_t *target, double *traj_dst, double *vel_dst) {
+// Shared set-up of nls_pool_set_downsample (linear) and
+// nls_pool_set_downsample_fft (spectral crop).
+int set_downsample(nls_pool *P, int32_t s, const int32_t *target, double *traj_dst, double *vel_dst, bool fft) {
   if (!P || !target || !traj_dst) return fail(NLS_ERR_INVALID_ARG, "null argument");
   if (s < 0 || s >= P->max_slots || !P->hs[s].used) return fail(NLS_ERR_INVALID_ARG, "bad slot");
   SlotHost &h = P->hs[s];
@@ -1631,18 +1642,35 @@ int nls_pool_set_downsample(nls_pool *P, int32_t s, const int32_t *target, doubl
   const int comps = P->cplx ? 2 : 1, nfields = P->cplx ? 1 : 2;
   int rc = make_ds_tables(dim, shape, tgt, L, comps, nfields, g, idx, y);
   if (rc) return rc;
-  // one allocation: staging frame (all fields), distances, indices
+  FftDsPlan plan;
+  std::vector<double> mats;
+  if (fft && !fft_ds_tables(dim, shape, tgt, plan, mats))
+    return fail(NLS_ERR_INVALID_ARG, "spectral downsampling needs 1 <= target <= source extent on every axis");
+  // one allocation: staging frame (all fields), then the linear tables or the
+  // spectral matrices and two complex work buffers
   const size_t stage_b = sizeof(double) * (size_t)(g.dst_field * nfields);
-  const size_t y_b = sizeof(double) * y.size(), i_b = sizeof(int32_t) * idx.size();
+  const size_t y_b = fft ? 0 : sizeof(double) * y.size(), i_b = fft ? 0 : sizeof(int32_t) * idx.size();
+  const size_t m_b = fft ? sizeof(double) * mats.size() : 0;
+  const size_t w_b = fft ? sizeof(double) * 2 * (size_t)plan.work_complex : 0;
   char *dev = nullptr;
-  CK(cudaMalloc((void **)&dev, stage_b + y_b + i_b));
-  double *dy = (double *)(dev + stage_b);
-  int32_t *di = (int32_t *)(dev + stage_b + y_b);
-  CK(cudaMemcpyAsync(dy, y.data(), y_b, cudaMemcpyHostToDevice, P->stream));
-  CK(cudaMemcpyAsync(di, idx.data(), i_b, cudaMemcpyHostToDevice, P->stream));
-  g.y = dy;
-  g.idx = di;
+  CK(cudaMalloc((void **)&dev, stage_b + y_b + i_b + m_b + 2 * w_b));
+  if (fft) {
+    double *dm = (double *)(dev + stage_b);
+    CK(cudaMemcpyAsync(dm, mats.data(), m_b, cudaMemcpyHostToDevice, P->stream));
+    plan.mats = dm;
+    plan.work[0] = (double *)(dev + stage_b + m_b);
+    plan.work[1] = (double *)(dev + stage_b + m_b + w_b);
+  } else {
+    double *dy = (double *)(dev + stage_b);
+    int32_t *di = (int32_t *)(dev + stage_b + y_b);
+    CK(cudaMemcpyAsync(dy, y.data(), y_b, cudaMemcpyHostToDevice, P->stream));
+    CK(cudaMemcpyAsync(di, idx.data(), i_b, cudaMemcpyHostToDevice, P->stream));
+    g.y = dy;
+    g.idx = di;
+  }
   h.ds = true;
+  h.ds_fft = fft;
+  h.ds_plan = plan;
   h.ds_geom = g;
   h.ds_frame = g.dst_field * nfields;
   h.ds_dev = dev;
@@ -1656,6 +1684,48 @@ int nls_pool_set_downsample(nls_pool *P, int32_t s, const int32_t *target, doubl
   const double *frame0 = P->snap + P->sd[s].snap_off;
   rc = enqueue_downsample(P, h, frame0, 0, P->stream);
   if (rc) return rc;
+  return NLS_OK;
+}
+
+int nls_pool_set_downsample(nls_pool *P, int32_t s, const int32_t *target, double *traj_dst, double *vel_dst) {
+  return set_downsample(P, s, target, traj_dst, vel_dst, false);
+}
+
+int nls_pool_set_downsample_fft(nls_pool *P, int32_t s, const int32_t *target, double *traj_dst,
+                                double *vel_dst) {
+  return set_downsample(P, s, target, traj_dst, vel_dst, true);
+}
+
+int nls_downsample_fft(int32_t dim, const int64_t *shape, const int64_t *target, int32_t frames, int32_t is_complex,
+                       const double *in, double *out) {
+  if (!shape || !target || !in || !out || (dim != 2 && dim != 3) || frames < 0)
+    return fail(NLS_ERR_INVALID_ARG, "bad downsampling arguments");
+  FftDsPlan plan;
+  std::vector<double> mats;
+  if (!fft_ds_tables(dim, shape, target, plan, mats))
+    return fail(NLS_ERR_INVALID_ARG, "spectral downsampling needs 1 <= target <= source extent on every axis");
+  if (frames == 0) return NLS_OK;
+  const int comps = is_complex ? 2 : 1;
+  int64_t src = comps, dst = comps;
+  for (int d = 0; d < dim; ++d) {
+    src *= shape[d];
+    dst *= target[d];
+  }
+  const size_t in_b = sizeof(double) * (size_t)(src * frames), out_b = sizeof(double) * (size_t)(dst * frames);
+  const size_t m_b = sizeof(double) * mats.size(), w_b = sizeof(double) * 2 * (size_t)plan.work_complex;
+  char *dev = nullptr;
+  CK(cudaMalloc((void **)&dev, in_b + out_b + m_b + 2 * w_b));
+  double *din = (double *)dev, *dout = (double *)(dev + in_b);
+  plan.mats = (const double *)(dev + in_b + out_b);
+  plan.work[0] = (double *)(dev + in_b + out_b + m_b);
+  plan.work[1] = (double *)(dev + in_b + out_b + m_b + w_b);
+  cudaError_t e = cudaMemcpy(din, in, in_b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy((void *)plan.mats, mats.data(), m_b, cudaMemcpyHostToDevice);
+  for (int f = 0; f < frames && e == cudaSuccess; ++f)
+    e = fft_ds_field(plan, din + (int64_t)f * src, !is_complex, dout + (int64_t)f * dst, !is_complex, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, out_b, cudaMemcpyDeviceToHost);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
   return NLS_OK;
 }
 

@@ -36,6 +36,7 @@ SYMBOLS = [
     "nls_pool_step_timed", "nls_set_device", "nls_host_alloc", "nls_host_free",
     "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
     "nls_pool_set_downsample", "nls_downsample_linear", "nls_pool_snapshots_ready",
+    "nls_pool_set_downsample_fft", "nls_downsample_fft",
 ]
 
 
@@ -114,6 +115,8 @@ def lib() -> ctypes.CDLL:
         "nls_pool_set_downsample": [vp, i32, ip, dp, dp],
         "nls_downsample_linear": [i32, ctypes.POINTER(i64), ctypes.POINTER(i64), dp, i32, i32, dp, dp],
         "nls_pool_snapshots_ready": [vp, i32, ip],
+        "nls_pool_set_downsample_fft": [vp, i32, ip, dp, dp],
+        "nls_downsample_fft": [i32, ctypes.POINTER(i64), ctypes.POINTER(i64), i32, i32, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

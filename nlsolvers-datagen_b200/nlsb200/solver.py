@@ -138,6 +138,37 @@ def downsample_interpolation_3d(u, target_shape, Lx, Ly, Lz):
     return _downsample(u, target_shape, (Lx, Ly, Lz))
 
 
+def _downsample_fft(u, target_shape):
+    u = np.asarray(u)
+    cplx = np.iscomplexobj(u)
+    dim = u.ndim - 1
+    tgt = tuple(int(t) for t in target_shape)
+    if len(tgt) != dim:
+        raise ValueError(f"target shape {tgt} does not match {dim}-D frames")
+    src = np.ascontiguousarray(u, dtype=np.complex128 if cplx else np.float64)
+    out = np.empty((u.shape[0],) + tgt, dtype=src.dtype)
+    shape = (ctypes.c_int64 * 3)(*u.shape[1:])
+    tg = (ctypes.c_int64 * 3)(*tgt)
+    check(lib().nls_downsample_fft(dim, shape, tg, u.shape[0], int(cplx), _dptr(src.view(np.float64)),
+                                   _dptr(out.view(np.float64))))
+    return out.astype(u.dtype)
+
+
+def downsample_fft(u, target_shape):
+    """Drop-in for the reference's downsample_fft (scripts/downsampling.py:10-35):
+    u (frames, n0, n1), centred crop of the orthonormal spectrum to
+    target_shape, computed on the GPU in FP64."""
+    assert np.ndim(u) == 3 and len(target_shape) == 2
+    return _downsample_fft(u, target_shape)
+
+
+def downsample_fft_3d(u, target_shape):
+    """Drop-in for the reference's downsample_fft_3d
+    (scripts/downsampling.py:147-178): u (frames, n0, n1, n2)."""
+    assert np.ndim(u) == 4 and len(target_shape) == 3
+    return _downsample_fft(u, target_shape)
+
+
 def _dptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -309,13 +340,17 @@ class Pool:
         check(lib().nls_pool_set_diagnostics(self._p, slot, _dptr(info.diag)))
         return info.diag
 
-    def set_downsample(self, slot: int, target_shape):
+    def set_downsample(self, slot: int, target_shape, mode: str = "linear"):
         """Downsample every snapshot of `slot` on the device to `target_shape`
         (array-axis order) before its copy to the host, as the reference's HDF5
         aggregation does on the host (see nls_pool_set_downsample). Call before
         the slot's first step; returns (ds_traj, ds_vel) of shape
         (ns,) + target_shape, filled as snapshots complete (ds_vel is None for
-        the NLSE); the slot's full-size outputs then hold snapshot 0 only."""
+        the NLSE); the slot's full-size outputs then hold snapshot 0 only.
+        mode "linear": linear interpolation (nls_pool_set_downsample); "fft":
+        the spectral crop (nls_pool_set_downsample_fft)."""
+        if mode not in ("linear", "fft"):
+            raise ValueError(f"unknown downsampling mode {mode!r}")
         info = self.slots[slot]
         spec = info.spec
         tgt = tuple(int(t) for t in target_shape)
@@ -324,7 +359,8 @@ class Pool:
         traj = np.zeros((spec.ns,) + tgt, dtype=np.complex128 if spec.complex else np.float64)
         vel = None if spec.complex else np.zeros((spec.ns,) + tgt)
         t32 = (ctypes.c_int32 * 3)(*(tgt + (1,) * (3 - len(tgt))))
-        check(lib().nls_pool_set_downsample(self._p, slot, t32, _dptr(traj.view(np.float64)), _dptr(vel)))
+        fn = lib().nls_pool_set_downsample_fft if mode == "fft" else lib().nls_pool_set_downsample
+        check(fn(self._p, slot, t32, _dptr(traj.view(np.float64)), _dptr(vel)))
         info.ds_traj, info.ds_vel = traj, vel
         return traj, vel
 

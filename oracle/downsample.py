@@ -1,12 +1,15 @@
-"""CPU restatement (numpy) of the reference's linear-interpolation
-downsampling, scripts/downsampling.py:68-103 (downsample_interpolation) and
+"""CPU restatement (numpy) of the reference's snapshot downsampling: the
+spectral crop (downsample_fft below) and the linear interpolation,
+scripts/downsampling.py:68-103 (downsample_interpolation) and
 :215-257 (downsample_interpolation_3d), which its HDF5 aggregation applies to
 every snapshot (scripts/aggregate_single.py:61-76).
 
-Test infrastructure only (the tests use it as the checker; the product path is
-the CUDA kernel k_downsample). Pinned: equal bitwise to the reference's own
-outputs on tests/golden/downsampling.npz (made by
-tests/golden/make_downsampling_golden.py from the reference functions).
+Test infrastructure only (the tests use it as the checker; the product paths
+are the CUDA kernels k_downsample and k_zgemm_strided). Pinned: the linear
+form equal bitwise to the reference's own outputs on
+tests/golden/downsampling.npz, the spectral form within 1e-13 of them on
+tests/golden/fft_downsampling.npz (both made by tests/golden/make_*_golden.py
+from the reference functions).
 
 Array axis d has the source grid linspace(-L_d, L_d, n_d) and the target grid
 linspace(-L_d, L_d, t_d), L = (Lx, Ly[, Lz]) in array-axis order as the
@@ -67,3 +70,23 @@ def downsample_interpolation(u, target_shape, L):
                         acc = acc + v[idx[0] + b0, idx[1] + b1, idx[2] + b2] * ((w0 * w1) * w2)
         out[f] = acc
     return out
+
+
+def downsample_fft(u, target_shape):
+    """CPU restatement of the reference's spectral downsampling,
+    scripts/downsampling.py:10-35 (downsample_fft, frames of 2-D arrays) and
+    :147-178 (downsample_fft_3d): per array axis the orthonormal DFT, fftshift,
+    the crop of the centred target bins from (n - t) // 2, ifftshift and the
+    orthonormal inverse DFT; real inputs keep the real part. u: (frames,) +
+    source shape; target_shape: the frame axes' target extents."""
+    u = np.asarray(u)
+    cplx = np.iscomplexobj(u)
+    axes = tuple(range(1, u.ndim))
+    ft = np.fft.fftshift(np.fft.fftn(u.astype(np.complex128), axes=axes, norm="ortho"), axes=axes)
+    sl = [slice(None)]
+    for n, t in zip(u.shape[1:], target_shape):
+        s = (n - t) // 2
+        sl.append(slice(s, s + t))
+    crop = np.fft.ifftshift(ft[tuple(sl)], axes=axes)
+    out = np.fft.ifftn(crop, axes=axes, norm="ortho")
+    return (out if cplx else out.real).astype(u.dtype)

@@ -82,4 +82,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NLS_REFERENCE_DIR", "")
+    if not ref:
+        sys.exit("usage: %s REFERENCE_CHECKOUT (or set NLS_REFERENCE_DIR)" % sys.argv[0])
+    main(ref)
