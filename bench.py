@@ -382,19 +382,30 @@ def run_reference(args, ws, rank, budget_s=150.0):
     return 0
 
 
-def serving_leg(count=24, rate_hz=8.0, steps=(200, 600), seed=5):
+SERVE_RATES_HZ = (2.0, 8.0, 32.0)
+
+
+def serving_leg(count=24, rates=SERVE_RATES_HZ, steps=(500, 5000), seed=5, budget_gib=8.0):
     """The serving mix (requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
-    64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D; Poisson arrivals), shortened
-    to `steps` per request so that it runs in seconds: latency percentiles
-    (arrival to last snapshot on the host) and aggregate throughput."""
+    64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D, 500-5000 steps each, Poisson
+    arrivals) at each rate of `rates`: latency percentiles (arrival to last
+    snapshot on the host) and aggregate throughput (all requests' grid-point
+    steps over the run's wall time). Admission by an 8 GiB device-memory
+    budget shared by the class pools; page-locked client snapshot buffers."""
     from nlsb200 import serve
-    reqs = serve.mixed_requests(count, rate_hz, seed=seed, steps=steps)
-    srv = serve.Server(serve.default_classes(reqs, max_slots=16), chunk=10)
-    st = srv.run(reqs, timeout_s=300)
-    srv.close()
-    out = st.summary()
-    out.update({"requests": count, "rate_hz": rate_hz, "steps_per_request": list(steps),
-                "classes": sorted({r.cls for r in reqs}), "unit": UNIT})
+    out = {"rates": [], "requests_per_rate": count, "steps_per_request": list(steps), "unit": UNIT,
+           "memory_budget_bytes": int(budget_gib * (1 << 30)), "snapshots_per_request": 5}
+    for i, rate in enumerate(rates):
+        reqs = serve.mixed_requests(count, rate, seed=seed + i, steps=steps, ns=5, pinned=True)
+        srv = serve.Server(serve.default_classes(reqs, max_slots=32), chunk=20,
+                           memory_budget=int(budget_gib * (1 << 30)))
+        st = srv.run(reqs, timeout_s=600)
+        srv.close()
+        row = st.summary()
+        row.update({"rate_hz": rate, "classes": sorted({r.cls for r in reqs}),
+                    "gp_steps": st.gp_steps})
+        out["rates"].append(row)
+        del reqs
     return out
 
 

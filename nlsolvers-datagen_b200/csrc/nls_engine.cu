@@ -407,6 +407,7 @@ struct SlotHost {
   bool reg_traj = false, reg_vel = false;
   cudaEvent_t copy_done[NF] = {nullptr, nullptr};
   bool copy_pending[NF] = {false, false};
+  cudaEvent_t last_step_done = nullptr;  // recorded after the slot's last step (i = nt - 1) is enqueued
   bool needs_ss2 = false;  // SEWI: first step is a Strang step
   int ring_cnt = 0;
   double *diag = nullptr;  // ns x 4 diagnostics (host), or null
@@ -1170,6 +1171,9 @@ int pool_step_once(nls_pool *P) {
       int rc = issue_copies(P, h, P->sd[s], h.step);
       if (rc) return rc;
       h.step += 1;
+      // after its last step nothing queued later touches the slot's memory (the
+      // tables drop it); poll and release wait on this event, not the stream
+      if (h.step > h.nt - 1) CK(cudaEventRecord(h.last_step_done, P->stream));
     }
   return NLS_OK;
 }
@@ -1467,6 +1471,8 @@ int nls_pool_admit(nls_pool *P, const nls_problem *p, const double *u0, const do
   for (int f = 0; f < NF; ++f)
     if (cudaEventCreateWithFlags(&h.copy_done[f], cudaEventDisableTiming) != cudaSuccess)
       return fail(NLS_ERR_CUDA, "event");
+  if (cudaEventCreateWithFlags(&h.last_step_done, cudaEventDisableTiming) != cudaSuccess)
+    return fail(NLS_ERR_CUDA, "event");
   SlotDesc &d = P->sd[s];
   std::memset(&d, 0, sizeof(d));
   const double dx = 2 * p->Lx / (p->nx - 1), dy = 2 * p->Ly / (p->ny - 1);
@@ -1553,6 +1559,11 @@ int nls_pool_poll(nls_pool *P, int32_t s, int32_t *steps_done, int32_t *finished
   if (steps_done) *steps_done = h.step - 1;
   if (finished) {
     bool fin = h.step > h.nt - 1;
+    if (fin) {
+      const cudaError_t e = cudaEventQuery(h.last_step_done);
+      if (e == cudaErrorNotReady) fin = false;
+      else if (e != cudaSuccess) return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
+    }
     for (int f = 0; f < NF && fin; ++f) {
       if (h.copy_pending[f]) {
         cudaError_t e = cudaEventQuery(h.copy_done[f]);
@@ -1593,8 +1604,12 @@ int nls_pool_release(nls_pool *P, int32_t s) {
     if (h.copy_pending[f]) CK(cudaEventSynchronize(h.copy_done[f]));
     if (h.copy_done[f]) cudaEventDestroy(h.copy_done[f]);
   }
-  // the slot's memory is reused by later admissions only after queued steps
-  CK(cudaStreamSynchronize(P->stream));
+  // the slot's memory is reused by later admissions only after its queued
+  // steps: after its last step those are done when last_step_done is (later
+  // steps never include it); a slot released early waits for the stream
+  if (h.step > h.nt - 1) CK(cudaEventSynchronize(h.last_step_done));
+  else CK(cudaStreamSynchronize(P->stream));
+  if (h.last_step_done) cudaEventDestroy(h.last_step_done);
   if (h.reg_traj) cudaHostUnregister(h.traj);
   if (h.reg_vel) cudaHostUnregister(h.vel);
   if (h.reg_diag) cudaHostUnregister(h.diag);
@@ -1897,6 +1912,7 @@ int nls_pool_destroy(nls_pool *P) {
     if (!h.used) continue;
     for (int f = 0; f < NF; ++f)
       if (h.copy_done[f]) cudaEventDestroy(h.copy_done[f]);
+    if (h.last_step_done) cudaEventDestroy(h.last_step_done);
     if (h.reg_traj) cudaHostUnregister(h.traj);
     if (h.reg_vel) cudaHostUnregister(h.vel);
     if (h.reg_diag) cudaHostUnregister(h.diag);

@@ -3,12 +3,21 @@
 The reference runs one trajectory per process invocation (its launchers call a
 driver binary per run, scripts/real_launcher_2d.py:143-170). Here one process
 keeps one pool per request class (method, dim, Krylov dimension, precision)
-and runs continuous batching. Requests arrive over time and join their class's
-pool as soon as it has room (first come, first served within a class). All
-running trajectories of a pool advance together. A trajectory leaves its pool
-when its last snapshot has reached the host. Every pool has its own CUDA
-streams, so stepping several pools back to back overlaps their work on the
-GPU.
+and runs continuous batching:
+  - requests arrive over time and are queued per class (first come, first
+    served within a class);
+  - admission is by device memory: every class draws from one budget of
+    device bytes, and a request is admitted when its bytes (its padded grid
+    points times its class's bytes per point: fields, Krylov basis, snapshot
+    frames) fit in what the running requests leave free and its pool has a
+    free slot;
+  - all running trajectories of a pool advance together; a trajectory leaves
+    when its last snapshot has reached the host and its last step ran, and
+    its bytes return to the budget;
+  - every pool is driven by its own host thread on its own CUDA streams, so the
+    classes step independently and their work overlaps on the GPU; a thread
+    waits for each chunk of steps it queued before it admits, polls and queues
+    the next, so a new request waits at most one chunk.
 
 Latency of a request = completion time - arrival time (wall clock).
 """
@@ -16,14 +25,17 @@ from __future__ import annotations
 
 import math
 import os
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from .solver import FP32, KG_GAUTSCHI, NLSE_SS2, SP4_SV, Pool, Spec
 from . import workloads as W
+from .solver import FP32, FP64, KG_GAUTSCHI, KG_SV, NLSE_SEWI, NLSE_SS2, SP4_GAUTSCHI, SP4_SV, Pool, Spec, pinned_empty
+
+NF = 2  # device snapshot frames per trajectory (the engine's double buffer)
 
 
 @dataclass
@@ -40,10 +52,40 @@ class Request:
     t_done: float = math.nan
     slot: int = -1
     traj: np.ndarray | None = None
+    out_traj: np.ndarray | None = None  # client-owned output buffers (e.g. page-locked)
+    out_vel: np.ndarray | None = None
 
     @property
     def gp_steps(self) -> int:
         return self.spec.n * (self.spec.nt - 1)
+
+
+def bytes_per_point(method: int, k: int, precision: int) -> int:
+    """Device bytes a pool of this class holds per padded grid point (the
+    allocations of nls_pool_create): u_hi, u_lo, m, c, the increment d (real
+    methods), the Stormer-Verlet ping-pong buffer, the SEWI history and work
+    fields, the Krylov basis (two sequences, one for SS2) and NF FP64
+    snapshot frames of (u, v) or complex u."""
+    cplx = method in (NLSE_SS2, NLSE_SEWI)
+    rsz = 8 if precision == FP64 else 4
+    esz = rsz * (2 if cplx else 1)
+    b = 2 * esz + 2 * rsz
+    if not cplx:
+        b += rsz
+    if method in (KG_SV, SP4_SV):
+        b += esz
+    if method == NLSE_SEWI:
+        b += 4 * esz
+    if method in (KG_GAUTSCHI, SP4_GAUTSCHI, NLSE_SS2, NLSE_SEWI):
+        b += esz * (1 if method == NLSE_SS2 else 2) * (k - 1)
+    return b + 8 * 2 * NF
+
+
+def padded_points(spec) -> int:
+    """Points a trajectory occupies in its pool: rows padded to 32 elements,
+    the region rounded to 256 points."""
+    n = ((spec.nx + 31) // 32 * 32) * spec.ny * (spec.nz if spec.dim == 3 else 1)
+    return (n + 255) // 256 * 256
 
 
 @dataclass
@@ -52,8 +94,12 @@ class PoolClass:
     dim: int
     k: int
     precision: int = FP32
-    capacity_points: int = 1 << 22
     max_slots: int = 32
+    capacity_points: int | None = None  # None: the whole memory budget in this class's points
+
+    @property
+    def bytes_per_point(self) -> int:
+        return bytes_per_point(self.method, self.k, self.precision)
 
 
 @dataclass
@@ -62,6 +108,7 @@ class ServeStats:
     wall_s: float
     gp_steps: int
     latencies_s: list = field(default_factory=list)
+    peak_bytes: int = 0
 
     def summary(self) -> dict:
         lat = np.array(self.latencies_s) * 1e3
@@ -69,83 +116,207 @@ class ServeStats:
                 "gp_steps_per_s": self.gp_steps / self.wall_s if self.wall_s > 0 else 0.0,
                 "p50_ms": float(np.percentile(lat, 50)) if lat.size else None,
                 "p99_ms": float(np.percentile(lat, 99)) if lat.size else None,
-                "mean_ms": float(lat.mean()) if lat.size else None}
+                "mean_ms": float(lat.mean()) if lat.size else None,
+                "peak_device_bytes": self.peak_bytes}
 
 
 class Server:
-    """Pools by class name; `run(requests)` serves them in arrival order."""
+    """Pools by class name; `run(requests)` serves them in arrival order.
 
-    def __init__(self, classes: dict[str, PoolClass], chunk: int = 10, make_pool=None):
+    memory_budget: device bytes shared by all classes' running requests.
+    threads: one host thread per pool (False: one thread visits the pools in
+    turn, the order deterministic, for tests with stand-in pools)."""
+
+    def __init__(self, classes: dict[str, PoolClass], chunk: int = 20, memory_budget: int = 8 << 30,
+                 make_pool=None, threads: bool = True):
         self.classes = classes
         self.chunk = chunk
-        make_pool = make_pool or (lambda pc: Pool(pc.method, pc.dim, pc.k, pc.precision, pc.capacity_points,
-                                                  pc.max_slots))
+        self.budget = int(memory_budget)
+        self.threads = threads
+
+        def default_pool(pc):
+            cap = pc.capacity_points or max(self.budget // pc.bytes_per_point, 1 << 16)
+            return Pool(pc.method, pc.dim, pc.k, pc.precision, cap, pc.max_slots)
+        make_pool = make_pool or default_pool
         self.pools = {name: make_pool(pc) for name, pc in classes.items()}
 
     def close(self):
         for p in self.pools.values():
             p.close()
 
+    def request_bytes(self, r: Request) -> int:
+        return padded_points(r.spec) * self.classes[r.cls].bytes_per_point
+
     def run(self, requests: list[Request], clock=time.perf_counter, timeout_s: float = 600.0,
             out_dir: str | None = None) -> ServeStats:
         """Serve `requests`; with out_dir, every request's snapshots are also
         streamed to out_dir/req<rid>_traj.npy (and _vel.npy for KG / phi^4) as
         they reach the host, in the reference drivers' .npy layout."""
-        pending = deque(sorted(requests, key=lambda r: r.arrival))
-        queues = {name: deque() for name in self.classes}
-        running = {name: {} for name in self.classes}  # slot -> request
-        done = []
-        t0 = clock()
-        while len(done) < len(requests):
-            now = clock() - t0
-            if now > timeout_s:
-                raise TimeoutError(f"serving run exceeded {timeout_s} s ({len(done)}/{len(requests)} done)")
-            while pending and pending[0].arrival <= now:
-                r = pending.popleft()
-                queues[r.cls].append(r)
-            for name, q in queues.items():
-                pool = self.pools[name]
-                while q:
-                    r = q[0]
-                    out = None
-                    if out_dir:
-                        base = os.path.join(out_dir, f"req{r.rid:05d}")
-                        out = (base + "_traj.npy", None if r.spec.complex else base + "_vel.npy")
-                    slot = pool.admit(r.spec, r.u0, r.v0, r.m, r.c, **({"out_npy": out} if out else {}))
-                    if slot is None:
-                        break  # full: the request waits for a release
-                    q.popleft()
-                    r.slot, r.t_admit = slot, clock() - t0
-                    running[name][slot] = r
-            active = [name for name in self.classes if running[name]]
-            if not active:
-                if pending:  # idle until the next arrival
-                    time.sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.05)))
-                continue
-            for name in active:
-                self.pools[name].step(self.chunk)
-            for name in active:
-                pool = self.pools[name]
-                for slot, r in list(running[name].items()):
-                    _, finished = pool.poll(slot)
-                    if finished:
-                        info = pool.release(slot)
-                        r.traj = info.traj
-                        r.t_done = clock() - t0
-                        del running[name][slot]
-                        done.append(r)
-        wall = clock() - t0
-        return ServeStats(completed=len(done), wall_s=wall, gp_steps=sum(r.gp_steps for r in done),
-                          latencies_s=[r.t_done - r.arrival for r in done])
+        for r in requests:
+            if self.request_bytes(r) > self.budget:
+                raise ValueError(f"request {r.rid} needs {self.request_bytes(r)} device bytes, more than the "
+                                 f"budget of {self.budget}")
+        st = _RunState(self, requests, clock, out_dir)
+        if self.threads:
+            st.run_threaded(timeout_s)
+        else:
+            st.run_sequential(timeout_s)
+        wall = clock() - st.t0
+        return ServeStats(completed=len(st.done), wall_s=wall, gp_steps=sum(r.gp_steps for r in st.done),
+                          latencies_s=[r.t_done - r.arrival for r in st.done], peak_bytes=st.peak)
+
+
+class _RunState:
+    """Queues, running sets and the device-byte ledger of one Server.run."""
+
+    def __init__(self, srv: Server, requests, clock, out_dir):
+        self.srv, self.clock, self.out_dir = srv, clock, out_dir
+        self.n = len(requests)
+        self.pending = deque(sorted(requests, key=lambda r: r.arrival))
+        self.queues = {name: deque() for name in srv.classes}
+        self.running = {name: {} for name in srv.classes}  # slot -> request
+        self.done = []
+        self.used = 0
+        self.peak = 0
+        self.lock = threading.Lock()
+        self.cond = threading.Condition(self.lock)
+        self.error = None
+        self.t0 = clock()
+
+    def now(self):
+        return self.clock() - self.t0
+
+    def release_arrivals(self):
+        now = self.now()
+        while self.pending and self.pending[0].arrival <= now:
+            r = self.pending.popleft()
+            self.queues[r.cls].append(r)
+
+    def admit(self, name):
+        """Admit queued requests of class `name` while their bytes fit in the
+        budget and the pool takes them (FIFO: the head waits for room)."""
+        pool = self.srv.pools[name]
+        q = self.queues[name]
+        while True:
+            with self.lock:
+                if not q:
+                    return
+                r = q[0]
+                need = self.srv.request_bytes(r)
+                if self.used + need > self.srv.budget:
+                    return
+                self.used += need  # reserved before the (slow) upload
+                self.peak = max(self.peak, self.used)
+            out = None
+            if self.out_dir:
+                base = os.path.join(self.out_dir, f"req{r.rid:05d}")
+                out = (base + "_traj.npy", None if r.spec.complex else base + "_vel.npy")
+            kw = {}
+            if out:
+                kw["out_npy"] = out
+            if r.out_traj is not None:
+                kw["traj"] = r.out_traj
+                if r.out_vel is not None:
+                    kw["vel"] = r.out_vel
+            slot = pool.admit(r.spec, r.u0, r.v0, r.m, r.c, **kw)
+            with self.lock:
+                if slot is None:  # no free slot or pool capacity: wait for a release
+                    self.used -= need
+                    return
+                q.popleft()
+                r.slot, r.t_admit = slot, self.now()
+                self.running[name][slot] = r
+
+    def collect(self, name):
+        pool = self.srv.pools[name]
+        for slot, r in list(self.running[name].items()):
+            _, finished = pool.poll(slot)
+            if finished:
+                info = pool.release(slot)
+                with self.cond:
+                    r.traj = info.traj
+                    r.t_done = self.now()
+                    del self.running[name][slot]
+                    self.done.append(r)
+                    self.used -= self.srv.request_bytes(r)
+                    self.cond.notify_all()
+
+    def service(self, name, sync):
+        """One round of class `name`: admit, step a chunk, poll and release."""
+        self.admit(name)
+        if not self.running[name]:
+            return False
+        pool = self.srv.pools[name]
+        pool.step(self.srv.chunk)
+        if sync:
+            pool.sync()
+        self.collect(name)
+        return True
+
+    def run_sequential(self, timeout_s):
+        while len(self.done) < self.n:
+            if self.now() > timeout_s:
+                raise TimeoutError(f"serving run exceeded {timeout_s} s ({len(self.done)}/{self.n} done)")
+            self.release_arrivals()
+            busy = False
+            for name in self.srv.classes:
+                busy |= self.service(name, sync=False)
+            if not busy and self.pending:  # idle until the next arrival
+                time.sleep(max(0.0, min(self.pending[0].arrival - self.now(), 0.05)))
+
+    def _worker(self, name):
+        try:
+            while True:
+                with self.cond:
+                    if self.error is not None or len(self.done) >= self.n:
+                        return
+                if not self.service(name, sync=True):
+                    with self.cond:
+                        self.cond.wait(timeout=0.002)
+        except BaseException as ex:  # surfaced by the dispatching thread
+            with self.cond:
+                self.error = ex
+                self.cond.notify_all()
+
+    def run_threaded(self, timeout_s):
+        workers = [threading.Thread(target=self._worker, args=(name,), daemon=True) for name in self.srv.classes]
+        for w in workers:
+            w.start()
+        try:
+            while True:
+                with self.cond:
+                    self.release_arrivals()
+                    self.cond.notify_all()
+                    if self.error is not None or len(self.done) >= self.n:
+                        break
+                    if self.now() > timeout_s:
+                        self.error = TimeoutError(f"serving run exceeded {timeout_s} s "
+                                                  f"({len(self.done)}/{self.n} done)")
+                        break
+                    wait = 0.005
+                    if self.pending:
+                        wait = max(0.0, min(self.pending[0].arrival - self.now(), wait))
+                    self.cond.wait(timeout=wait)
+        finally:
+            with self.cond:
+                if self.error is None and len(self.done) < self.n:
+                    self.error = RuntimeError("serving run stopped")
+                self.cond.notify_all()
+            for w in workers:
+                w.join(timeout=120)
+        if self.error is not None and len(self.done) < self.n:
+            raise self.error
 
 
 def mixed_requests(count: int, rate_hz: float, seed: int = 0, steps=(500, 5000), scale: float = 1.0,
-                   ns: int = 10) -> list[Request]:
+                   ns: int = 10, pinned: bool = False) -> list[Request]:
     """The serving mix: requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
     64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D (u_tt = Lu + u - u^3 + sigma xi,
     sigma ~ U(0.05, 0.5), discrete noise sigma xi / sqrt(dt dx^d) with Philox
     keyed by (seed, step, point)); Poisson arrivals at rate_hz; step counts
-    uniform in `steps`. `scale` shrinks the grid edges (for short runs)."""
+    uniform in `steps`. `scale` shrinks the grid edges (for short runs).
+    pinned: each request brings page-locked snapshot buffers (a client that
+    allocated them ahead), so admission registers no memory."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -174,20 +345,25 @@ def mixed_requests(count: int, rate_hz: float, seed: int = 0, steps=(500, 5000),
             spec.rm, spec.r0 = 0.0, sigma / math.sqrt(spec.dt * dx ** 2)
             m = np.ones(u0.shape)
         c = None
-        out.append(Request(i, kind, t, spec, u0, v0, m, c))
+        req = Request(i, kind, t, spec, u0, v0, m, c)
+        if pinned:
+            dt = np.complex128 if spec.complex else np.float64
+            req.out_traj = pinned_empty((spec.ns,) + spec.shape, dt)
+            if not spec.complex:
+                req.out_vel = pinned_empty((spec.ns,) + spec.shape)
+        out.append(req)
     return out
 
 
 def default_classes(requests: list[Request], max_slots: int = 32) -> dict[str, PoolClass]:
-    """One pool per class, sized for its largest request x max_slots."""
+    """One pool per class present in `requests` (KG 2-D and 3-D with k = 10,
+    NLSE 2-D SS2 with k = 12, phi^4 2-D Stormer-Verlet), up to max_slots
+    trajectories each; their points come from the shared memory budget."""
     method = {"kg2d": (KG_GAUTSCHI, 2, 10), "nlse2d": (NLSE_SS2, 2, 12), "kg3d": (KG_GAUTSCHI, 3, 10),
               "phi4_2d": (SP4_SV, 2, 3)}
     out = {}
     for name, (meth, dim, k) in method.items():
         rs = [r for r in requests if r.cls == name]
-        if not rs:
-            continue
-        big = max(((r.spec.nx + 31) // 32 * 32) * r.spec.ny * (r.spec.nz if dim == 3 else 1) for r in rs)
-        slots = min(max_slots, len(rs))
-        out[name] = PoolClass(meth, dim, k, FP32, capacity_points=slots * (big + 256), max_slots=slots)
+        if rs:
+            out[name] = PoolClass(meth, dim, k, FP32, max_slots=min(max_slots, len(rs)))
     return out

@@ -49,9 +49,9 @@ class Clock:
         return self.t
 
 
-def _req(rid, cls, arrival, nt):
+def _req(rid, cls, arrival, nt, nx=10):
     from nlsb200.serve import Request
-    spec = types.SimpleNamespace(nt=nt, n=100, tag=rid)
+    spec = types.SimpleNamespace(nt=nt, n=100, tag=rid, nx=nx, ny=10, nz=1, dim=2, complex=False)
     return Request(rid, cls, arrival, spec, None, None, None)
 
 
@@ -67,7 +67,7 @@ def test_fifo_admission_latency_and_throughput():
 
     classes = {"a": serve.PoolClass(method=0, dim=2, k=10, max_slots=2),
                "b": serve.PoolClass(method=1, dim=2, k=10, max_slots=1)}
-    srv = serve.Server(classes, chunk=10, make_pool=make_pool)
+    srv = serve.Server(classes, chunk=10, make_pool=make_pool, threads=False)
     reqs = [_req(0, "a", 0.0, 101), _req(1, "a", 0.0, 51), _req(2, "a", 0.0, 31),
             _req(3, "b", 0.0, 21), _req(4, "b", 0.0, 21)]
     st = srv.run(reqs, clock=clock)
@@ -97,3 +97,45 @@ def test_mixed_requests_shapes_and_phi4_form():
             assert 0.05 <= sigma <= 0.5
     classes = serve.default_classes(reqs)
     assert set(classes) == {q.cls for q in reqs}
+
+
+def test_admission_by_shared_device_memory_budget():
+    """Two classes share one budget of two requests' bytes: the class-b
+    requests wait, with slots free in their pool, until a class-a request
+    finishes and its bytes return to the budget."""
+    from nlsb200 import serve
+    clock = Clock()
+
+    classes = {"a": serve.PoolClass(method=0, dim=2, k=10, max_slots=4),
+               "b": serve.PoolClass(method=0, dim=2, k=10, max_slots=4)}
+    # a 10 x 10 grid pads to 32 x 10 = 320 -> 512 points
+    per = 512 * serve.bytes_per_point(0, 10, serve.FP32)
+    srv = serve.Server(classes, chunk=10, make_pool=lambda pc: FakePool(pc.max_slots, clock), threads=False,
+                       memory_budget=2 * per)
+    reqs = [_req(0, "a", 0.0, 101), _req(1, "a", 0.0, 51), _req(2, "b", 0.0, 31), _req(3, "b", 0.0, 21)]
+    st = srv.run(reqs, clock=clock)
+    assert st.completed == 4 and st.peak_bytes == 2 * per
+    r = {q.rid: q for q in reqs}
+    assert r[0].t_admit == r[1].t_admit == 0.0
+    assert r[2].t_admit >= r[1].t_done - 1e-12   # waits for bytes, not for a slot
+    assert r[3].t_admit >= min(r[0].t_done, r[2].t_done) - 1e-12
+
+
+def test_bytes_per_point_follows_the_pool_allocations():
+    from nlsb200 import serve
+    from nlsb200.solver import FP32, FP64, KG_GAUTSCHI, NLSE_SEWI, NLSE_SS2, SP4_SV
+    # KG FP32, k = 9: u_hi, u_lo, m, c, d (20 B) + V 2 x 8 x 4 B + 2 snapshot frames of (u, v) FP64
+    assert serve.bytes_per_point(KG_GAUTSCHI, 9, FP32) == 20 + 64 + 32
+    # NLSE SS2 complex64, k = 12: 2 x 8 + 2 x 4 + 1 x 11 x 8 + 32
+    assert serve.bytes_per_point(NLSE_SS2, 12, FP32) == 24 + 88 + 32
+    assert serve.bytes_per_point(NLSE_SEWI, 12, FP32) == 24 + 4 * 8 + 2 * 11 * 8 + 32
+    assert serve.bytes_per_point(SP4_SV, 3, FP64) == 16 + 16 + 8 + 8 + 32
+
+
+def test_oversized_request_is_rejected():
+    from nlsb200 import serve
+    clock = Clock()
+    classes = {"a": serve.PoolClass(method=0, dim=2, k=10, max_slots=1)}
+    srv = serve.Server(classes, make_pool=lambda pc: FakePool(1, clock), threads=False, memory_budget=1000)
+    with pytest.raises(ValueError):
+        srv.run([_req(0, "a", 0.0, 11)], clock=clock)
