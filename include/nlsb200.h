@@ -33,6 +33,7 @@ extern "C" {
 #define NLS_ERR_STATE -7       /* call not valid in the current state */
 #define NLS_ERR_NUMERIC -8     /* eigensolver did not converge / non-finite state */
 #define NLS_ERR_IO -9          /* file or .npy format error (CLI helpers) */
+#define NLS_ERR_TIMEOUT -10    /* a bounded device wait ran out; the step did not complete */
 
 /* Integrators (device/drivers/CMakeLists.txt:15-31). */
 #define NLS_KG_GAUTSCHI 0  /* kg_gautschi_{2d,3d}_dev: KGESolverDevice::step (kg_dev.hpp:97) */
@@ -224,6 +225,21 @@ int nls_pool_time_pass(nls_pool *pool, int32_t j, int32_t iters, float *ms, int6
    the pool's stream around them (waits for completion): *ms = device time of
    all nsteps steps. */
 int nls_pool_step_timed(nls_pool *pool, int32_t nsteps, float *ms);
+/* 2-D FP32 Gautschi pools (KG / phi^4, c == 1, k <= 16): 1 runs a step as one
+   kernel, in which warps claim the work items of the launch sequence (first
+   pass, Lanczos passes, f(T), final pass, ghost ring) in stage order and wait,
+   bounded, for the stages each item needs; 0 (default) runs the launch
+   sequence (two slot groups on parallel graph branches), which measures
+   faster on 64 x 300^2. Results are bitwise the same. Other pools ignore the
+   setting. */
+int nls_pool_set_step_kernel(nls_pool *pool, int32_t one_kernel);
+/* Bounds of the one-kernel step's waits: a wait gives up after `polls` polls
+   (about 0.1 us each, default 2^22); the step then ends incomplete and the
+   next nls_pool_sync returns NLS_ERR_TIMEOUT. stall_stage >= 0 (for testing)
+   makes every wait of that stage (0: first pass, j: Lanczos pass j, k-1: f(T),
+   k: final pass, k+1: ghost ring) wait for a count nothing reaches, so that
+   its waits must run out; -1: off. */
+int nls_pool_set_wait_limit(nls_pool *pool, int64_t polls, int32_t stall_stage);
 /* Launch counts of the most recent step: kernels launched per step. */
 int nls_pool_kernels_per_step(nls_pool *pool, int32_t *count);
 int nls_pool_destroy(nls_pool *pool);

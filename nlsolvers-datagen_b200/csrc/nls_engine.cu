@@ -507,6 +507,14 @@ struct nls_pool {
   int ring_blocks = 1;
   int kernels_per_step = 0;
   int device = 0;
+  // one-kernel step (k2_step_dyn) of the 2-D FP32 Gautschi families
+  bool dyn_on = false;          // nls_pool_set_step_kernel
+  bool dyn_step = false;        // the current tables run it
+  int *d_dyn = nullptr;         // its counters and stage flags (2 + 3 max_slots ints)
+  int dyn_grid = 0;             // resident blocks (SMs x blocks per SM)
+  long long dyn_spin_limit = 1LL << 22;  // polls before a wait gives up (nls_pool_set_wait_limit)
+  int dyn_stall = -1;           // testing: stage whose waits cannot be met
+  int graph_dyn = -1;
 };
 
 struct nls_handle {
@@ -559,7 +567,8 @@ void pool_free_device(nls_pool *P) {
                   P->first.d_ntt2, P->main2.d_tiles, P->main2.d_ntiles, P->main2.d_list,
                   P->main2.d_nlist, P->main2.d_lt, P->main2.d_nlt1, P->main2.d_nlt2, P->main2.d_tt,
                   P->main2.d_ntt1, P->main2.d_ntt2, P->zeros, P->d_diag_part, P->d_diag_out, P->d_diag_ticket,
-                  P->main.d_ft, P->main.d_nft, P->main2.d_ft, P->main2.d_nft, P->first.d_ft, P->first.d_nft};
+                  P->main.d_ft, P->main.d_nft, P->main2.d_ft, P->main2.d_nft, P->first.d_ft, P->first.d_nft,
+                  P->d_dyn};
   for (void *b : bufs)
     if (b) cudaFree(b);
 }
@@ -651,7 +660,14 @@ int rebuild_tables(nls_pool *P) {
     const SlotHost &h = P->hs[s];
     if (h.used && h.step <= h.nt - 1 && !(h.needs_ss2 && h.step == 1)) ++nmain;
   }
-  P->split = P->split_on && nmain >= 2;
+  // the one-kernel step needs no second group: its items of every slot
+  // already interleave; it runs 2-D FP32 Gautschi steps with c == 1, k <= 16
+  bool any_c = false;
+  for (int s = 0; s < P->max_slots; ++s)
+    if (P->hs[s].used && P->hs[s].step <= P->hs[s].nt - 1 && P->hs[s].prob.has_c) any_c = true;
+  P->dyn_step = P->dyn_on && P->dim == 2 && P->prec == NLS_FP32 && !any_c && P->k <= 16 &&
+                (P->method == NLS_KG_GAUTSCHI || P->method == NLS_SP4_GAUTSCHI);
+  P->split = P->split_on && nmain >= 2 && !P->dyn_step;
   int64_t load[2] = {0, 0};
   for (int s = 0; s < P->max_slots; ++s) {
     SlotHost &h = P->hs[s];
@@ -761,7 +777,11 @@ int rebuild_tables(nls_pool *P) {
     }
     if (P->dim == 2) {
       T->ft.clear();
-      for (int sidx : T->list) slot_tiles(P, sidx, P->sd[sidx], T->ft, P->segf2);
+      for (int sidx : T->list) {
+        const size_t f0 = T->ft.size();
+        slot_tiles(P, sidx, P->sd[sidx], T->ft, P->segf2);
+        P->sd[sidx].ft_count = (int)(T->ft.size() - f0);
+      }
       T->ft_live = (int)T->ft.size();
       if (T->ft_live > T->fcap || !T->d_ft) {
         if (T->d_ft) cudaFree(T->d_ft);
@@ -959,9 +979,46 @@ int enqueue_step(nls_pool *P, const TileSet &T, bool mode_first, cudaStream_t st
   return NLS_OK;
 }
 
+// The one-kernel step (k2_step_dyn): the stage flags and item counter zeroed,
+// then one launch of resident blocks over the main tables.
+template <int KP> cudaError_t launch_step_dyn(const StepArgs &a, const DynArgs &d, int grid, cudaStream_t st) {
+  k2_step_dyn<KP><<<grid, 32 * WPB, 0, st>>>(a, d);
+  return cudaGetLastError();
+}
+int enqueue_dyn(nls_pool *P) {
+  const TileSet &T = P->main;
+  StepArgs a = base_args(P, T, 0);
+  // kg_single.cuh:103-111: cos(tau sqrt A) u and sinc^2(tau sqrt A) g(u), A = -L
+  a.nseq = 2;
+  a.op_sign = -1.0;
+  a.fkind[0] = FK_COS_SQRT;
+  a.fkind[1] = FK_SINC2_SQRT;
+  a.incr[0] = 1;
+  a.incr[1] = 0;
+  a.tsc[0][0] = 1.0;
+  a.tsc[1][0] = 1.0;
+  DynArgs d;
+  d.lt = T.d_lt;
+  d.nlt1 = T.d_nlt1;
+  d.nlt2 = T.d_nlt2;
+  d.ft = T.d_ft;
+  d.nft = T.d_nft;
+  d.sync = P->d_dyn;
+  d.max_slots = P->max_slots;
+  d.stall_stage = P->dyn_stall;
+  d.spin_limit = P->dyn_spin_limit;
+  CK(cudaMemsetAsync(P->d_dyn, 0, sizeof(int) * (2 + 3 * (size_t)P->max_slots), P->stream));
+  if (P->k <= 8) CK(launch_step_dyn<8>(a, d, P->dyn_grid, P->stream));
+  else if (P->k <= 12) CK(launch_step_dyn<12>(a, d, P->dyn_grid, P->stream));
+  else CK(launch_step_dyn<16>(a, d, P->dyn_grid, P->stream));
+  P->kernels_per_step = 1;
+  return NLS_OK;
+}
+
 // The main step: one launch sequence, or (two groups) a fork onto stream2, the
 // two groups' sequences side by side, and a join back onto the pool stream.
 int enqueue_main(nls_pool *P) {
+  if (P->dyn_step) return enqueue_dyn(P);
   if (!P->split) return enqueue_step(P, P->main, false, P->stream, 0);
   CK(cudaEventRecord(P->ev_fork, P->stream));
   CK(cudaStreamWaitEvent(P->stream2, P->ev_fork, 0));
@@ -982,7 +1039,7 @@ int run_main_step(nls_pool *P) {
   if (!P->gexec || P->graph_tiles != P->main.cap || P->graph_ring != P->ring_blocks ||
       P->graph_hc != P->step_hc || P->graph_part != (void *)P->part ||
       P->graph_lcap != P->main.lcap || P->graph_tcap != P->main.tcap || P->graph_split != sp ||
-      P->graph_fcap != P->main.fcap ||
+      P->graph_fcap != P->main.fcap || P->graph_dyn != (int)P->dyn_step ||
       (sp && (P->graph_tiles2 != P->main2.cap || P->graph_lcap2 != P->main2.lcap ||
               P->graph_tcap2 != P->main2.tcap || P->graph_fcap2 != P->main2.fcap))) {
     if (P->gexec) {
@@ -1013,6 +1070,7 @@ int run_main_step(nls_pool *P) {
     P->graph_tcap2 = P->main2.tcap;
     P->graph_fcap = P->main.fcap;
     P->graph_fcap2 = P->main2.fcap;
+    P->graph_dyn = (int)P->dyn_step;
   }
   CK(cudaGraphLaunch(P->gexec, P->stream));
   return NLS_OK;
@@ -1250,6 +1308,7 @@ const char *nls_strerror(int code) {
   case NLS_ERR_STATE: return "invalid state";
   case NLS_ERR_NUMERIC: return "numerical failure";
   case NLS_ERR_IO: return "I/O error";
+  case NLS_ERR_TIMEOUT: return "device wait timed out";
   }
   return "unknown error";
 }
@@ -1371,6 +1430,20 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_diag_part, sizeof(double) * max_slots * DIAG_BLOCKS * 4);
   if (!rc) rc = al((void **)&P->d_diag_out, sizeof(double) * max_slots * 4);
   if (!rc) rc = al((void **)&P->d_diag_ticket, sizeof(int) * max_slots);
+  if (!rc) rc = al((void **)&P->d_dyn, sizeof(int) * (2 + 3 * (size_t)max_slots));
+  if (!rc && dim == 2 && precision == NLS_FP32 && (method == NLS_KG_GAUTSCHI || method == NLS_SP4_GAUTSCHI)) {
+    // resident blocks of the one-kernel step: its items are claimed in order,
+    // so any grid completes; one full wave keeps every SM busy
+    int nsm = 0, per = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, P->device);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k <= 8 ? (const void *)k2_step_dyn<8>
+                                                              : k <= 12 ? (const void *)k2_step_dyn<12>
+                                                                        : (const void *)k2_step_dyn<16>,
+                                                        32 * WPB, 0);
+    if (e != cudaSuccess) rc = fail(NLS_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
+    P->dyn_grid = std::max(1, nsm * std::max(per, 1));
+  }
   for (TileSet *T : {&P->main, &P->main2, &P->first}) {
     if (!rc) rc = al((void **)&T->d_ntt1, sizeof(int));
     if (!rc) rc = al((void **)&T->d_ntt2, sizeof(int));
@@ -1792,6 +1865,9 @@ int nls_pool_sync(nls_pool *P) {
   CK(cudaMemcpy(st.data(), P->d_state, sizeof(SlotState) * P->max_slots, cudaMemcpyDeviceToHost));
   for (int s = 0; s < P->max_slots; ++s) {
     if (!P->hs[s].used || st[s].status == 0) continue;
+    if (st[s].status == -10)
+      return fail(NLS_ERR_TIMEOUT, "slot " + std::to_string(s) + ": a wait of the one-kernel step ran out "
+                  "(the step did not complete)");
     if (st[s].status == -9)
       return fail(NLS_ERR_NUMERIC, "slot " + std::to_string(s) + " diverged: non-finite Lanczos coefficients"
                   " (with NLSE SEWI, the reference operand order, sewi_variant 0, grows without bound;"
@@ -1831,6 +1907,23 @@ int nls_pool_set_final_segment(nls_pool *P, int32_t rows) {
   if (P->dim != 2) return fail(NLS_ERR_INVALID_ARG, "the final-pass segment applies to 2-D pools");
   P->segf2 = rows;
   P->tables_dirty = true;
+  return NLS_OK;
+}
+
+int nls_pool_set_step_kernel(nls_pool *P, int32_t one_kernel) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  if (one_kernel != 0 && one_kernel != 1) return fail(NLS_ERR_INVALID_ARG, "one_kernel must be 0 or 1");
+  P->dyn_on = one_kernel == 1;
+  P->tables_dirty = true;
+  return NLS_OK;
+}
+
+int nls_pool_set_wait_limit(nls_pool *P, int64_t polls, int32_t stall_stage) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  if (polls < 0 || stall_stage < -1) return fail(NLS_ERR_INVALID_ARG, "polls >= 0 and stall_stage >= -1");
+  P->dyn_spin_limit = polls;
+  P->dyn_stall = stall_stage;
+  P->graph_dyn = -1;  // the limits are launch arguments: capture the step again
   return NLS_OK;
 }
 

@@ -929,13 +929,14 @@ __device__ bool ftri_fast(int k, const double *d, const double *e, int lane, int
 // so all indices are static) and applies each Givens rotation to its own row
 // `lane` of the eigenvector matrix immediately: no shared memory, no per-sweep
 // synchronisation.
-template <typename E, int KP>
-__global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
-  pdl_entry();
+// f(T)e1 of (slot list entry gw / nseq, sequence gw % nseq) by one warp. DYN:
+// inside the one-kernel step, where the warp then publishes stage k of that
+// (slot, sequence) in `done` once every lane's coefficients are visible.
+template <typename E, int KP, bool DYN>
+__device__ __forceinline__ void ftri_reg_body(const StepArgs &a, int gw, int *done) {
   constexpr bool CP = Traits<E>::cplx;
   using R = typename Traits<E>::R;
   const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int li = gw / a.nseq, sq = gw % a.nseq;
   if (li >= *a.nslot_list) return;
   const int slot = a.slot_list[li];
@@ -1149,6 +1150,17 @@ __global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
     if (!finite) a.state[slot].status = -9;
     else if (status) a.state[slot].status = -8;
   }
+  if (DYN) {
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(done + slot * 2 + sq), "r"(k) : "memory");
+  }
+}
+
+template <typename E, int KP>
+__global__ void __launch_bounds__(128) k_ftri_reg(StepArgs a) {
+  pdl_entry();
+  ftri_reg_body<E, KP, false>(a, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), nullptr);
 }
 
 #include "nls_kernels_tail.cuh"

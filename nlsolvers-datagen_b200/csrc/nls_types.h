@@ -25,7 +25,7 @@ struct SlotDesc {
   int32_t variant;           // NLSE SEWI operand order: 0 reference, 1 corrected
   int32_t tile_begin2, tile_count2;  // tiles of the block-table passes (2-D TMA, 3-D FP32)
   int32_t nl_kind;           // nonlinearity (NLS_NL_*: 0 polynomial / cubic)
-  int32_t pad_;
+  int32_t ft_count;          // 2-D: tiles of the slot in the final-pass table
 };
 
 // Mutable per-slot state on the device (advanced by the boundary kernel).

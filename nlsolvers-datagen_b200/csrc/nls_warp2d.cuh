@@ -29,6 +29,19 @@ template <typename E> __device__ __forceinline__ V16<E> ld16(const E *p) {
   memcpy(&r, &w, 16);
   return r;
 }
+// L2 load (ld.global.cg) for data another warp of the same launch may have
+// written: the one-kernel step (k2_step_dyn) reads the Krylov vectors and
+// fields that way; ld16's read-only path serves data of earlier launches.
+template <typename E> __device__ __forceinline__ V16<E> ld16cg(const E *p) {
+  V16<E> r;
+  const uint4 w = __ldcg(reinterpret_cast<const uint4 *>(p));
+  memcpy(&r, &w, 16);
+  return r;
+}
+template <bool CG, typename E> __device__ __forceinline__ V16<E> ld16x(const E *p) {
+  if constexpr (CG) return ld16cg(p);
+  else return ld16(p);
+}
 template <typename E> __device__ __forceinline__ void st16(E *p, const V16<E> &r) {
   uint4 w;
   memcpy(&w, &r, 16);
@@ -55,9 +68,9 @@ struct Strip {
   __device__ __forceinline__ long long addr(int r) const { return off + (long long)r * pitch + col0; }
 };
 
-template <typename E>
+template <typename E, bool CG = false>
 __device__ __forceinline__ V16<E> load_row(const E *base, const Strip &S, int r) {
-  if (S.lane_in && S.row_ok(r)) return ld16(base + S.addr(r));
+  if (S.lane_in && S.row_ok(r)) return ld16x<CG>(base + S.addr(r));
   return vzero<E>();
 }
 
@@ -630,6 +643,10 @@ template <typename R> struct FinRow<FIN_KG, R> {
     const long long o = S.addr(r);
     return Fld{ld16((const R *)a.f.u_hi + o), ld16((const R *)a.f.u_lo + o), ld16((const R *)a.f.d + o)};
   }
+  static __device__ __forceinline__ Fld load_cg(const StepArgs &a, const Strip &S, int r) {
+    const long long o = S.addr(r);
+    return Fld{ld16cg((const R *)a.f.u_hi + o), ld16cg((const R *)a.f.u_lo + o), ld16cg((const R *)a.f.d + o)};
+  }
   static __device__ __forceinline__ void apply(const StepArgs &a, const SlotDesc &s, const Strip &S,
                                                int step, int r, Fld f, const V16<R> *y) {
     constexpr int N = V16<R>::N;
@@ -780,18 +797,25 @@ template <typename R> struct FinRow<FIN_SEWI_B, Cx<R>> {
 // (the warps of a block may belong to different slots).
 // Real FP32: built for four blocks per SM (128 registers; a few spill), which
 // measured faster than three blocks at 167 registers.
-template <typename E, int NSEQ, int FIN, bool HC>
-__global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 1) k2_final(StepArgs a) {
-  pdl_entry();
+// One final-pass tile (warp wt of `tiles`). W: this warp's coefficient slice
+// in shared memory. DYN: inside the one-kernel step, where the Krylov vectors
+// and fields of this step were written by other warps of the same launch
+// (L2 loads instead of the read-only path).
+template <typename E, int NSEQ, int FIN, bool HC, bool DYN>
+__device__ __forceinline__ void final2_body(const StepArgs &a, const TileDesc *tiles, int ntiles, int wt,
+                                            typename Traits<E>::R (*W)[KMAX][2]) {
   using R = typename Traits<E>::R;
   using FR = FinRow<FIN, E>;
   constexpr int NB = 8;
-  __shared__ R Wsh[WPB][NSEQ][KMAX][2];
-  WARP_TILE_PROLOGUE
+  const int lane = threadIdx.x & 31;
+  if (wt >= ntiles) return;
+  const TileDesc t = tiles[wt];
+  const SlotDesc &s = a.slots[t.slot];
+  const Strip S = make_strip<V16<E>::N>(s, t, lane);
+  const int step = a.state[t.slot].step;
   const int kv = a.kv;
   const R opsc = R(a.op_sign * s.inv_h2);
   const R *cf = (const R *)a.f.c;
-  const int wib = threadIdx.x >> 5;
   const E *VL[NSEQ];
   R lr[NSEQ], li[NSEQ];
 #pragma unroll
@@ -806,8 +830,8 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
       li[sq] = R(F.lam_i);
     }
     // lanes >= kv store zeros: the batched loop reads up to NB entries past kv-2
-    Wsh[wib][sq][lane][0] = lane < kv ? coef_w<R>(F, lane, false) : R(0);
-    Wsh[wib][sq][lane][1] = lane < kv ? coef_w<R>(F, lane, true) : R(0);
+    W[sq][lane][0] = lane < kv ? coef_w<R>(F, lane, false) : R(0);
+    W[sq][lane][1] = lane < kv ? coef_w<R>(F, lane, true) : R(0);
   }
   __syncwarp();
   const bool io = S.out_lane;
@@ -816,9 +840,9 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
   const int r0 = t.p0, r1 = t.p1;
 #pragma unroll
   for (int sq = 0; sq < NSEQ; ++sq) {
-    Lo[sq] = load_row(VL[sq], S, r0 - 1);
-    Lp[sq] = load_row(VL[sq], S, r0);
-    Ln1[sq] = load_row(VL[sq], S, r0 + 1);
+    Lo[sq] = load_row<E, DYN>(VL[sq], S, r0 - 1);
+    Lp[sq] = load_row<E, DYN>(VL[sq], S, r0);
+    Ln1[sq] = load_row<E, DYN>(VL[sq], S, r0 + 1);
   }
   if constexpr (HC) {
     cw[1] = load_crow<E>(cf, S, r0 - 1);
@@ -832,17 +856,20 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
     CRow<E> cn2;
 #pragma unroll
     for (int sq = 0; sq < NSEQ; ++sq) {
-      Ln2[sq] = load_row(VL[sq], S, r + 2);
+      Ln2[sq] = load_row<E, DYN>(VL[sq], S, r + 2);
       const E *Vb = (const E *)a.V + (long long)(sq * kv) * a.vstride + S.addr(r);
 #pragma unroll
       for (int i = 0; i < NB; ++i)
         vb[sq][i] = (io && i < kv - 1)
-                        ? ld16((a.v0_u && sq == 0 && i == 0) ? (const E *)a.f.u_hi + S.addr(r) : Vb + (long long)i * a.vstride)
+                        ? ld16x<DYN>((a.v0_u && sq == 0 && i == 0) ? (const E *)a.f.u_hi + S.addr(r) : Vb + (long long)i * a.vstride)
                         : vzero<E>();
     }
     if constexpr (HC) cn2 = load_crow<E>(cf, S, r + 2);
     typename FR::Fld fld;
-    if (io) fld = FR::load(a, S, r);
+    if (io) {
+      if constexpr (DYN) fld = FR::load_cg(a, S, r);
+      else fld = FR::load(a, S, r);
+    }
     // ---- arithmetic
 #pragma unroll
     for (int sq = 0; sq < NSEQ; ++sq) {
@@ -863,13 +890,13 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
       V16<E> z;
       lap_any<E, R, HC>(S, r, Lm[sq], Lo[sq], Lp[sq], cw, opsc, z);
       V16<E> acc;
-      const R wlr = Wsh[wib][sq][kv - 1][0], wli = Wsh[wib][sq][kv - 1][1];
+      const R wlr = W[sq][kv - 1][0], wli = W[sq][kv - 1][1];
 #pragma unroll
       for (int e = 0; e < V16<E>::N; ++e)
         acc.v[e] = cfma(wlr, wli, Lo[sq].v[e], cmul(lr[sq], li[sq], z.v[e]));
 #pragma unroll
       for (int i = 0; i < NB; ++i) {
-        const R wr = Wsh[wib][sq][i][0], wi = Wsh[wib][sq][i][1];
+        const R wr = W[sq][i][0], wi = W[sq][i][1];
 #pragma unroll
         for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vb[sq][i].v[e], acc.v[e]);
       }
@@ -879,10 +906,10 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
           V16<E> vx[NB];
 #pragma unroll
           for (int i = 0; i < NB; ++i)
-            vx[i] = q0 + i < kv - 1 ? ld16(Vb + (long long)(q0 + i) * a.vstride) : vzero<E>();
+            vx[i] = q0 + i < kv - 1 ? ld16x<DYN>(Vb + (long long)(q0 + i) * a.vstride) : vzero<E>();
 #pragma unroll
           for (int i = 0; i < NB; ++i) {
-            const R wr = Wsh[wib][sq][q0 + i][0], wi = Wsh[wib][sq][q0 + i][1];
+            const R wr = W[sq][q0 + i][0], wi = W[sq][q0 + i][1];
 #pragma unroll
             for (int e = 0; e < V16<E>::N; ++e) acc.v[e] = cfma(wr, wi, vx[i].v[e], acc.v[e]);
           }
@@ -893,6 +920,15 @@ __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 
     }
     if (io && S.row_ok(r)) FR::apply(a, s, S, step, r, fld, y);
   }
+}
+
+template <typename E, int NSEQ, int FIN, bool HC>
+__global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 1) k2_final(StepArgs a) {
+  pdl_entry();
+  using R = typename Traits<E>::R;
+  __shared__ R Wsh[WPB][NSEQ][KMAX][2];
+  final2_body<E, NSEQ, FIN, HC, false>(a, a.tiles, *a.ntiles, blockIdx.x * WPB + (threadIdx.x >> 5),
+                                       Wsh[threadIdx.x >> 5]);
 }
 
 // ------------------------------------------------------- Stormer-Verlet
@@ -1497,13 +1533,33 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
   cp_async_wait<0>();
 }
 
-template <int MINB, bool LO = false>
-__global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
-  pdl_entry();
+// Publication of a stage of the one-kernel step: the release store of the
+// number of completed stages of (slot, sequence). The warp's own stores are
+// ordered before it by the release; the other warps' rows by their fence
+// before their ticket (dyn_fence_rows).
+__device__ __forceinline__ void dyn_publish(int *flag, int value) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(flag), "r"(value) : "memory");
+}
+// Every lane's stores of this item visible GPU-wide before the warp's ticket.
+__device__ __forceinline__ void dyn_fence_rows() {
+  __threadfence();
+  __syncwarp();
+}
+
+// One Lanczos pass tile: warp wt of the pass table `tiles` (ntiles entries,
+// lt_stride tiles per sequence section), pass j, this warp's cp.async cells
+// cellA / cellB of the two row rings. DYN: inside the one-kernel step (rows
+// fenced before the ticket; the last warp publishes stage j + 1 in `done`).
+template <bool LO, bool DYN>
+__device__ __forceinline__ void lz_f32c_body(const StepArgs &a, const TileDesc *tiles, int ntiles, int lt_stride,
+                                             int j, int wt, uint32_t cellA, uint32_t cellB, int *done) {
   using E = float;
-  __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
-  WARP_TILE_PROLOGUE
-  const int j = a.j, sq = t.local & 1;
+  const int lane = threadIdx.x & 31;
+  if (wt >= ntiles) return;
+  const TileDesc t = tiles[wt];
+  const SlotDesc &s = a.slots[t.slot];
+  const Strip S = make_strip<V16<E>::N>(s, t, lane);
+  const int sq = t.local & 1;
   const float opsc = float(a.op_sign * s.inv_h2);
   const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
   const double b0 = a.beta0[t.slot * 2 + sq];
@@ -1537,9 +1593,6 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
     OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
     xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
   }
-  const int wib = threadIdx.x >> 5;
-  const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&ring[wib][0][0][lane * 16]);
-  const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&ring[wib][1][0][lane * 16]);
   const bool ld = S.lane_in, io = S.out_lane;
   const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -1555,7 +1608,8 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
   double vals[ND];
 #pragma unroll
   for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
-  const int tc = s.tile_count, TT = *a.lt_stride;
+  const int tc = s.tile_count, TT = lt_stride;
+  if (DYN) dyn_fence_rows();
   if (warp_publish<ND>(vals, a.part + (long long)j * a.part_stride, wt, a.ticket + t.slot * 2 + sq,
                        tc, lane)) {
     const double *part = a.part + (long long)j * a.part_stride;
@@ -1567,8 +1621,19 @@ __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
     if (lane == 0) {
       a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
       a.ticket[t.slot * 2 + sq] = 0;
+      if (DYN) dyn_publish(done + t.slot * 2 + sq, j + 1);
     }
   }
+}
+
+template <int MINB, bool LO = false>
+__global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
+  pdl_entry();
+  __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  lz_f32c_body<LO, false>(a, a.tiles, *a.ntiles, *a.lt_stride, a.j, blockIdx.x * WPB + wib,
+                          (uint32_t)__cvta_generic_to_shared(&ring[wib][0][0][lane * 16]),
+                          (uint32_t)__cvta_generic_to_shared(&ring[wib][1][0][lane * 16]), nullptr);
 }
 
 // Packed FP32 first pass for KG / phi^4 (c == 1): one warp per (strip,
@@ -1669,10 +1734,18 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
 #undef NLSB_FIRST
 }
 
-static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
-  pdl_entry();
+// One first-pass tile (warp wt of the pass table). DYN: inside the one-kernel
+// step (rows fenced before the ticket; the last warp publishes stage 1).
+template <bool DYN>
+__device__ __forceinline__ void first_f32_body(const StepArgs &a, const TileDesc *tiles, int ntiles, int lt_stride,
+                                               int wt, int *done) {
   using E = float;
-  WARP_TILE_PROLOGUE
+  const int lane = threadIdx.x & 31;
+  if (wt >= ntiles) return;
+  const TileDesc t = tiles[wt];
+  const SlotDesc &s = a.slots[t.slot];
+  const Strip S = make_strip<V16<E>::N>(s, t, lane);
+  const int step = a.state[t.slot].step;
   const int sq = t.local & 1;
   const float opsc = float(a.op_sign * s.inv_h2);
   F4 OPx, xmiss;
@@ -1708,7 +1781,8 @@ static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
   double vals[ND];
 #pragma unroll
   for (int q = 0; q < ND; ++q) vals[q] = io ? acc[q] : 0.0;
-  const int tc = s.tile_count, TT = *a.lt_stride;
+  const int tc = s.tile_count, TT = lt_stride;
+  if (DYN) dyn_fence_rows();
   if (warp_publish<ND>(vals, a.part, wt, a.ticket + t.slot * 2 + sq, tc, lane)) {
     const double tot = warp_slot_total<ND>(a.part, sq * TT + s.tile_begin, tc, lane);
     double tv[ND];
@@ -1719,6 +1793,158 @@ static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
       a.scal[(t.slot * 2 + sq) * KMAX + 0] = lz_first<false>(tv, Eps<float>::v, b0);
       a.beta0[t.slot * 2 + sq] = b0;
       a.ticket[t.slot * 2 + sq] = 0;
+      if (DYN) dyn_publish(done + t.slot * 2 + sq, 1);
+    }
+  }
+}
+
+static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
+  pdl_entry();
+  first_f32_body<false>(a, a.tiles, *a.ntiles, *a.lt_stride, blockIdx.x * WPB + (threadIdx.x >> 5), nullptr);
+}
+
+// ------------------------------------------------------ one-kernel step
+// The 2-D FP32 Gautschi step (KG / phi^4, c == 1, k <= 16) as one launch. The
+// launch sequence (first pass, Lanczos passes j = 1..k-2, f(T), final pass,
+// ghost ring, step advance) becomes a list of work items in that stage order:
+//   stage 0      first-pass tiles              (pass table, both sequences)
+//   stage j      Lanczos pass j tiles          (pass table), j = 1..k-2
+//   stage k-1    f(T) solves                   (slot, sequence)
+//   stage k      final-pass tiles              (final table)
+//   stage k+1    ghost ring + step advance     (slot)
+// Warps claim items from one atomic counter, in that order, and run the same
+// per-tile code as the separate kernels. Before an item a warp waits until
+// the stage it needs has been published for its slot (and sequence): a
+// per-(slot, sequence) count of completed stages, written with release
+// semantics by the warp that finished the stage (the last ticket of a pass,
+// the f(T) warp), and a per-slot count of finished final tiles. An item only
+// waits for items of earlier stages, which running warps claimed before it,
+// so the step always completes; no wait runs unbounded: after `spin_limit`
+// polls the warp records a timeout (slot status -10), raises the abort flag
+// that makes every other wait give up, and the launch ends with the step
+// incomplete and the error reported to the host. The arithmetic and the
+// order of every reduction are those of the separate kernels, so results are
+// bitwise the same; the kernel boundaries between the dozen short launches of
+// a step (ramp-up and tail of each) disappear.
+struct DynArgs {
+  const TileDesc *lt;  // pass table (first pass and Lanczos passes)
+  const int *nlt1, *nlt2;
+  const TileDesc *ft;  // final-pass table
+  const int *nft;
+  int *sync;           // [0] item counter, [1] abort flag, [2, 2 + 2 max_slots) stages done per (slot, seq),
+                       // then finished final tiles per slot; zeroed before every launch
+  int max_slots;
+  int stall_stage;     // testing: the waits of this stage wait for a count nothing reaches (-1: off)
+  long long spin_limit;
+};
+
+// Wait until *flag >= target. Every lane polls with its own acquire load (one
+// warp instruction, one address), so each lane's later loads see what the
+// release published; the warp proceeds when all lanes saw the target. False
+// on timeout or abort: a timeout records status -10 in `state` and raises the
+// abort flag.
+__device__ __forceinline__ bool dyn_wait(const int *flag, int target, int *abort_flag, long long limit,
+                                         SlotState *state) {
+  const int lane = threadIdx.x & 31;
+  for (long long it = 0;; ++it) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(flag) : "memory");
+    if (__all_sync(0xffffffffu, v >= target)) return true;
+    if (__any_sync(0xffffffffu, *(volatile int *)abort_flag != 0)) return false;
+    if (it >= limit) {
+      if (lane == 0) {
+        state->status = -10;
+        atomicExch(abort_flag, 1);
+      }
+      __syncwarp();
+      return false;
+    }
+    __nanosleep(128);
+  }
+}
+
+// Ghost ring and step advance of one slot by one warp (k_ring and k_advance
+// for the KG real state), reading the final pass's values through L2.
+__device__ __forceinline__ void ring_kg_dyn_body(const StepArgs &a, int slot) {
+  const int lane = threadIdx.x & 31;
+  const SlotDesc &s = a.slots[slot];
+  const int step = a.state[slot].step;
+  const long long cnt = ring_count(s.dim, s.nx, s.ny, s.nz);
+  float *uh = (float *)a.f.u_hi, *ul = (float *)a.f.u_lo, *dd = (float *)a.f.d;
+  int fr;
+  const bool snap = snap_step(s, step, fr);
+  for (long long r = lane; r < cnt; r += 32) {
+    int x, y, z;
+    if (!ring_point(s, r, x, y, z)) continue;
+    const int cx = min(max(x, 1), s.nx - 2), cy = min(max(y, 1), s.ny - 2);
+    const long long eg = s.off + (long long)y * s.pitch + x;
+    const long long ec = s.off + (long long)cy * s.pitch + cx;
+    const float hc = __ldcg(uh + ec), lc = __ldcg(ul + ec);
+    const float hg = __ldcg(uh + eg), lg = __ldcg(ul + eg);
+    dd[eg] = ((hc - hg) + (lc - lg)) + __ldcg(dd + eg);
+    if (snap) a.f.snap[s.snap_off + (long long)fr * 2 * s.n + (long long)y * s.nx + x] = (double)hc + (double)lc;
+    uh[eg] = hc;
+    ul[eg] = lc;
+  }
+  __syncwarp();
+  if (lane == 0) a.state[slot].step = step + 1;
+}
+
+template <int KP>
+__global__ void __launch_bounds__(32 * WPB, 4) k2_step_dyn(StepArgs a, DynArgs d) {
+  __shared__ __align__(16) unsigned char smem[WPB][2][CPD][512];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&smem[wib][0][0][lane * 16]);
+  const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&smem[wib][1][0][lane * 16]);
+  float(*W)[KMAX][2] = reinterpret_cast<float(*)[KMAX][2]>(&smem[wib][0][0][0]);
+  int *counter = d.sync, *abort_flag = d.sync + 1, *done = d.sync + 2, *fin = d.sync + 2 + 2 * d.max_slots;
+  const int nl = *d.nlt2, nl1 = *d.nlt1, nf = *d.nft, ns = *a.nslot_list, k = a.k;
+  const long long n0 = nl, n1 = n0 + (long long)nl * (k - 2), n2 = n1 + 2LL * ns, n3 = n2 + nf,
+                  total = n3 + ns;
+  const int never = 0x7fffffff;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(counter, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= total) break;
+    if (*(volatile int *)abort_flag) break;
+    if (idx < n0) {  // stage 0
+      first_f32_body<true>(a, d.lt, nl, nl1, idx, done);
+      continue;
+    }
+    if (idx < n1) {  // stage j: Lanczos pass j
+      const int r = (int)(idx - n0), j = 1 + r / nl, w = r % nl;
+      const TileDesc t = d.lt[w];
+      const int key = t.slot * 2 + (t.local & 1);
+      if (!dyn_wait(done + key, d.stall_stage == j ? never : j, abort_flag, d.spin_limit, a.state + t.slot)) break;
+      if (j == 1) lz_f32c_body<true, true>(a, d.lt, nl, nl1, j, w, cellA, cellB, done);
+      else lz_f32c_body<false, true>(a, d.lt, nl, nl1, j, w, cellA, cellB, done);
+      continue;
+    }
+    if (idx < n2) {  // stage k-1: f(T) of (slot, sequence)
+      const int gw = (int)(idx - n1), slot = a.slot_list[gw >> 1];
+      const int key = slot * 2 + (gw & 1);
+      if (!dyn_wait(done + key, d.stall_stage == k - 1 ? never : k - 1, abort_flag, d.spin_limit, a.state + slot))
+        break;
+      ftri_reg_body<float, KP, true>(a, gw, done);
+      continue;
+    }
+    if (idx < n3) {  // stage k: final-pass tile
+      const int w = (int)(idx - n2);
+      const TileDesc t = d.ft[w];
+      const int tgt = d.stall_stage == k ? never : k;
+      if (!dyn_wait(done + t.slot * 2, tgt, abort_flag, d.spin_limit, a.state + t.slot)) break;
+      if (!dyn_wait(done + t.slot * 2 + 1, tgt, abort_flag, d.spin_limit, a.state + t.slot)) break;
+      final2_body<float, 2, FIN_KG, false, true>(a, d.ft, nf, w, W);
+      dyn_fence_rows();
+      if (lane == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;\n" ::"l"(fin + t.slot) : "memory");
+      continue;
+    }
+    {  // stage k+1: ghost ring and step advance of a slot
+      const int slot = a.slot_list[idx - n3];
+      const int tgt = d.stall_stage == k + 1 ? never : a.slots[slot].ft_count;
+      if (!dyn_wait(fin + slot, tgt, abort_flag, d.spin_limit, a.state + slot)) break;
+      ring_kg_dyn_body(a, slot);
     }
   }
 }

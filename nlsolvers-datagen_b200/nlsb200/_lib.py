@@ -17,7 +17,7 @@ NLS_OK = 0
 ERRORS = {
     -1: "invalid argument", -2: "shape mismatch", -3: "out of memory", -4: "CUDA error",
     -5: "no CUDA device", -6: "pool capacity exhausted", -7: "invalid state",
-    -8: "numerical failure", -9: "I/O error",
+    -8: "numerical failure", -9: "I/O error", -10: "device wait timed out",
 }
 NLS_ERR_CAPACITY = -6
 NLS_ERR_NO_DEVICE = -5
@@ -36,7 +36,7 @@ SYMBOLS = [
     "nls_pool_step_timed", "nls_set_device", "nls_host_alloc", "nls_host_free",
     "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
     "nls_pool_set_downsample", "nls_downsample_linear", "nls_pool_snapshots_ready",
-    "nls_pool_set_downsample_fft", "nls_downsample_fft",
+    "nls_pool_set_downsample_fft", "nls_downsample_fft", "nls_pool_set_step_kernel", "nls_pool_set_wait_limit",
 ]
 
 
@@ -117,6 +117,8 @@ def lib() -> ctypes.CDLL:
         "nls_pool_snapshots_ready": [vp, i32, ip],
         "nls_pool_set_downsample_fft": [vp, i32, ip, dp, dp],
         "nls_downsample_fft": [i32, ctypes.POINTER(i64), ctypes.POINTER(i64), i32, i32, dp, dp],
+        "nls_pool_set_step_kernel": [vp, i32],
+        "nls_pool_set_wait_limit": [vp, i64, i32],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -401,6 +401,15 @@ class Pool:
         check(lib().nls_pool_time_pass(self._p, j, iters, ctypes.byref(ms), ctypes.byref(pts)))
         return ms.value, pts.value
 
+    def set_step_kernel(self, one_kernel: bool):
+        """2-D FP32 Gautschi pools: run each step as one kernel (True) or as
+        the launch sequence (False, the default); see nls_pool_set_step_kernel."""
+        check(lib().nls_pool_set_step_kernel(self._p, 1 if one_kernel else 0))
+
+    def set_wait_limit(self, polls: int, stall_stage: int = -1):
+        """Bounds of the one-kernel step's device waits (nls_pool_set_wait_limit)."""
+        check(lib().nls_pool_set_wait_limit(self._p, int(polls), int(stall_stage)))
+
     def kernels_per_step(self) -> int:
         v = ctypes.c_int32()
         check(lib().nls_pool_kernels_per_step(self._p, ctypes.byref(v)))
