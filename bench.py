@@ -51,7 +51,7 @@ FALLBACK_HBM = 6650.0
 # DRAM bytes (read + write) per grid point of one Lanczos pass launch
 # (k2_lanczos1_f32c, j = 2, both sequences) in the ncu capture of
 # profiles/ncu_lanczos_pass_kg2d.md; algorithmic: 24 B per point.
-TRAFFIC_BYTES_PER_POINT_PASS = 17.85
+TRAFFIC_BYTES_PER_POINT_PASS = 17.94
 TIMED_REGION_S = 1.0
 
 

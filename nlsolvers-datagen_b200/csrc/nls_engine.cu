@@ -510,7 +510,7 @@ struct nls_pool {
   // one-kernel step (k2_step_dyn) of the 2-D FP32 Gautschi families
   bool dyn_on = false;          // nls_pool_set_step_kernel
   bool dyn_step = false;        // the current tables run it
-  int *d_dyn = nullptr;         // its counters and stage flags (2 + 3 max_slots ints)
+  int *d_dyn = nullptr;         // its counters and stage flags (DYN_SYNC_INTS(max_slots) ints)
   int dyn_grid = 0;             // resident blocks (SMs x blocks per SM)
   long long dyn_spin_limit = 1LL << 22;  // polls before a wait gives up (nls_pool_set_wait_limit)
   int dyn_stall = -1;           // testing: stage whose waits cannot be met
@@ -1007,7 +1007,7 @@ int enqueue_dyn(nls_pool *P) {
   d.max_slots = P->max_slots;
   d.stall_stage = P->dyn_stall;
   d.spin_limit = P->dyn_spin_limit;
-  CK(cudaMemsetAsync(P->d_dyn, 0, sizeof(int) * (2 + 3 * (size_t)P->max_slots), P->stream));
+  CK(cudaMemsetAsync(P->d_dyn, 0, sizeof(int) * (size_t)DYN_SYNC_INTS(P->max_slots), P->stream));
   if (P->k <= 8) CK(launch_step_dyn<8>(a, d, P->dyn_grid, P->stream));
   else if (P->k <= 12) CK(launch_step_dyn<12>(a, d, P->dyn_grid, P->stream));
   else CK(launch_step_dyn<16>(a, d, P->dyn_grid, P->stream));
@@ -1430,7 +1430,7 @@ int nls_pool_create(int32_t method, int32_t dim, int32_t k, int32_t precision,
   if (!rc) rc = al((void **)&P->d_diag_part, sizeof(double) * max_slots * DIAG_BLOCKS * 4);
   if (!rc) rc = al((void **)&P->d_diag_out, sizeof(double) * max_slots * 4);
   if (!rc) rc = al((void **)&P->d_diag_ticket, sizeof(int) * max_slots);
-  if (!rc) rc = al((void **)&P->d_dyn, sizeof(int) * (2 + 3 * (size_t)max_slots));
+  if (!rc) rc = al((void **)&P->d_dyn, sizeof(int) * (size_t)DYN_SYNC_INTS(max_slots));
   if (!rc && dim == 2 && precision == NLS_FP32 && (method == NLS_KG_GAUTSCHI || method == NLS_SP4_GAUTSCHI)) {
     // resident blocks of the one-kernel step: its items are claimed in order,
     // so any grid completes; one full wave keeps every SM busy

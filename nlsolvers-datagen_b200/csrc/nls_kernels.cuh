@@ -1153,7 +1153,7 @@ __device__ __forceinline__ void ftri_reg_body(const StepArgs &a, int gw, int *do
   if (DYN) {
     __threadfence();
     __syncwarp();
-    if (lane == 0) asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(done + slot * 2 + sq), "r"(k) : "memory");
+    if (lane == 0) asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(done + (slot * 2 + sq) * DYN_FS), "r"(k) : "memory");
   }
 }
 

@@ -6,6 +6,11 @@ namespace nlsb {
 
 constexpr int KMAX = 32;  // largest Krylov dimension (one warp per f(T) solve)
 
+// Synchronisation words of the one-kernel step, one 128-byte line each: with
+// hundreds of warps polling, flags that share a line load one L2 slice.
+#define DYN_FS 32
+#define DYN_SYNC_INTS(ms) ((2 + 3 * (ms)) * DYN_FS)
+
 // Immutable per-trajectory ("slot") description; lives in device memory.
 struct SlotDesc {
   int32_t dim, nx, ny, nz;   // full grid incl. ghost ring; nz = 1 in 2-D

@@ -1621,7 +1621,7 @@ __device__ __forceinline__ void lz_f32c_body(const StepArgs &a, const TileDesc *
     if (lane == 0) {
       a.scal[(t.slot * 2 + sq) * KMAX + j] = lz_from_dots<false>(tv, Eps<float>::v);
       a.ticket[t.slot * 2 + sq] = 0;
-      if (DYN) dyn_publish(done + t.slot * 2 + sq, j + 1);
+      if (DYN) dyn_publish(done + (t.slot * 2 + sq) * DYN_FS, j + 1);
     }
   }
 }
@@ -1793,7 +1793,7 @@ __device__ __forceinline__ void first_f32_body(const StepArgs &a, const TileDesc
       a.scal[(t.slot * 2 + sq) * KMAX + 0] = lz_first<false>(tv, Eps<float>::v, b0);
       a.beta0[t.slot * 2 + sq] = b0;
       a.ticket[t.slot * 2 + sq] = 0;
-      if (DYN) dyn_publish(done + t.slot * 2 + sq, 1);
+      if (DYN) dyn_publish(done + (t.slot * 2 + sq) * DYN_FS, 1);
     }
   }
 }
@@ -1831,25 +1831,29 @@ struct DynArgs {
   const int *nlt1, *nlt2;
   const TileDesc *ft;  // final-pass table
   const int *nft;
-  int *sync;           // [0] item counter, [1] abort flag, [2, 2 + 2 max_slots) stages done per (slot, seq),
-                       // then finished final tiles per slot; zeroed before every launch
+  int *sync;           // item counter, abort flag, stages done per (slot, seq), finished final tiles
+                       // per slot, each in a 128-byte line of its own (DYN_FS ints); zeroed before
+                       // every launch
   int max_slots;
   int stall_stage;     // testing: the waits of this stage wait for a count nothing reaches (-1: off)
   long long spin_limit;
 };
 
-// Wait until *flag >= target. Every lane polls with its own acquire load (one
-// warp instruction, one address), so each lane's later loads see what the
-// release published; the warp proceeds when all lanes saw the target. False
-// on timeout or abort: a timeout records status -10 in `state` and raises the
-// abort flag.
+// Wait until *flag >= target. Every lane polls with a relaxed load (one warp
+// instruction, one address) and, once all lanes saw the target, takes one
+// acquire load, so each lane's later loads see what the release published.
+// False on timeout or abort: a timeout records status -10 in `state` and
+// raises the abort flag.
 __device__ __forceinline__ bool dyn_wait(const int *flag, int target, int *abort_flag, long long limit,
                                          SlotState *state) {
   const int lane = threadIdx.x & 31;
   for (long long it = 0;; ++it) {
     int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(flag) : "memory");
-    if (__all_sync(0xffffffffu, v >= target)) return true;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(flag) : "memory");
+    if (__all_sync(0xffffffffu, v >= target)) {
+      asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(flag) : "memory");
+      return true;
+    }
     if (__any_sync(0xffffffffu, *(volatile int *)abort_flag != 0)) return false;
     if (it >= limit) {
       if (lane == 0) {
@@ -1897,7 +1901,9 @@ __global__ void __launch_bounds__(32 * WPB, 4) k2_step_dyn(StepArgs a, DynArgs d
   const uint32_t cellA = (uint32_t)__cvta_generic_to_shared(&smem[wib][0][0][lane * 16]);
   const uint32_t cellB = (uint32_t)__cvta_generic_to_shared(&smem[wib][1][0][lane * 16]);
   float(*W)[KMAX][2] = reinterpret_cast<float(*)[KMAX][2]>(&smem[wib][0][0][0]);
-  int *counter = d.sync, *abort_flag = d.sync + 1, *done = d.sync + 2, *fin = d.sync + 2 + 2 * d.max_slots;
+  constexpr int FS = DYN_FS;
+  int *counter = d.sync, *abort_flag = d.sync + DYN_FS, *done = d.sync + 2 * DYN_FS,
+      *fin = d.sync + (2 + 2 * d.max_slots) * DYN_FS;
   const int nl = *d.nlt2, nl1 = *d.nlt1, nf = *d.nft, ns = *a.nslot_list, k = a.k;
   const long long n0 = nl, n1 = n0 + (long long)nl * (k - 2), n2 = n1 + 2LL * ns, n3 = n2 + nf,
                   total = n3 + ns;
@@ -1916,7 +1922,7 @@ __global__ void __launch_bounds__(32 * WPB, 4) k2_step_dyn(StepArgs a, DynArgs d
       const int r = (int)(idx - n0), j = 1 + r / nl, w = r % nl;
       const TileDesc t = d.lt[w];
       const int key = t.slot * 2 + (t.local & 1);
-      if (!dyn_wait(done + key, d.stall_stage == j ? never : j, abort_flag, d.spin_limit, a.state + t.slot)) break;
+      if (!dyn_wait(done + key * FS, d.stall_stage == j ? never : j, abort_flag, d.spin_limit, a.state + t.slot)) break;
       if (j == 1) lz_f32c_body<true, true>(a, d.lt, nl, nl1, j, w, cellA, cellB, done);
       else lz_f32c_body<false, true>(a, d.lt, nl, nl1, j, w, cellA, cellB, done);
       continue;
@@ -1924,7 +1930,7 @@ __global__ void __launch_bounds__(32 * WPB, 4) k2_step_dyn(StepArgs a, DynArgs d
     if (idx < n2) {  // stage k-1: f(T) of (slot, sequence)
       const int gw = (int)(idx - n1), slot = a.slot_list[gw >> 1];
       const int key = slot * 2 + (gw & 1);
-      if (!dyn_wait(done + key, d.stall_stage == k - 1 ? never : k - 1, abort_flag, d.spin_limit, a.state + slot))
+      if (!dyn_wait(done + key * FS, d.stall_stage == k - 1 ? never : k - 1, abort_flag, d.spin_limit, a.state + slot))
         break;
       ftri_reg_body<float, KP, true>(a, gw, done);
       continue;
@@ -1933,17 +1939,17 @@ __global__ void __launch_bounds__(32 * WPB, 4) k2_step_dyn(StepArgs a, DynArgs d
       const int w = (int)(idx - n2);
       const TileDesc t = d.ft[w];
       const int tgt = d.stall_stage == k ? never : k;
-      if (!dyn_wait(done + t.slot * 2, tgt, abort_flag, d.spin_limit, a.state + t.slot)) break;
-      if (!dyn_wait(done + t.slot * 2 + 1, tgt, abort_flag, d.spin_limit, a.state + t.slot)) break;
+      if (!dyn_wait(done + t.slot * 2 * FS, tgt, abort_flag, d.spin_limit, a.state + t.slot)) break;
+      if (!dyn_wait(done + (t.slot * 2 + 1) * FS, tgt, abort_flag, d.spin_limit, a.state + t.slot)) break;
       final2_body<float, 2, FIN_KG, false, true>(a, d.ft, nf, w, W);
       dyn_fence_rows();
-      if (lane == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;\n" ::"l"(fin + t.slot) : "memory");
+      if (lane == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;\n" ::"l"(fin + t.slot * FS) : "memory");
       continue;
     }
     {  // stage k+1: ghost ring and step advance of a slot
       const int slot = a.slot_list[idx - n3];
       const int tgt = d.stall_stage == k + 1 ? never : a.slots[slot].ft_count;
-      if (!dyn_wait(fin + slot, tgt, abort_flag, d.spin_limit, a.state + slot)) break;
+      if (!dyn_wait(fin + slot * FS, tgt, abort_flag, d.spin_limit, a.state + slot)) break;
       ring_kg_dyn_body(a, slot);
     }
   }
