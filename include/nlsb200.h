@@ -202,6 +202,36 @@ int nls_pool_set_downsample_fft(nls_pool *pool, int32_t slot, const int32_t *tar
    target[0..dim-1]. Computed on the current device (synchronous). */
 int nls_downsample_fft(int32_t dim, const int64_t *shape, const int64_t *target, int32_t frames, int32_t is_complex,
                        const double *in, double *out);
+/* Coefficient fields m(x), c(x) of the reference's launchers on the device:
+   the formulas of scripts/m_fields_2d.py:14-145 and scripts/c_fields_2d.py:
+   12-166 on the grid x = linspace(-L, L, n), X[i][j] = x[i], Y[i][j] = x[j]
+   (n x n, C order). The caller draws the random parameters and noise arrays
+   (nlsb200.fields does it with numpy's global generator in the reference's
+   order); out receives the field. Gaussian filters (scipy.ndimage's, mode
+   reflect) take their 1-D weights w[taps] from the caller. params by kind:
+     1  m piecewise     m1, m2, boundary (0 circle, 1 square, 2 horizontal,
+                        3 vertical, 4 diagonal), boundary_param, smooth_width
+     2  m gradient      m0, gamma, epsilon                      (in: c)
+     3  m phase         m0, delta, shift_pixels                 (in: c)
+     4  m topological   m0, eta, lambda, taps, w...             (in: c)
+     5  m defects       m0, q, then q x (x0, y0, strength, width)
+     6  m quasiperiodic m0, q, then q x (kx, ky, amplitude, phase)
+     7  m multiscale    m0, q, then q x (amplitude, taps, w...) (in: q noises)
+     11 c periodic      base, amplitude, k
+     12 c piecewise     num_layers, base, contrast, layer_width
+     13 c sign-changing base, regions (0 checkerboard, 1 half space),
+                        cell_size, sharpness
+     14 c layered       base, q, then q x (nx, ny, amplitude, freq, phase)
+     15 c waveguide     base, guide_amplitude, q, points, then q x (width,
+                        curve x[points], curve y[points])
+     16 c quasiperiodic base, q, then q x (kx, ky, amplitude, phase)
+     17 c turbulent     base, intensity, q, then q x (amplitude, taps, w...)
+                        (in: q noises)
+   in: nin fields of n x n doubles as the kind needs (0 otherwise). Computed on
+   the current device (synchronous); agrees with the reference's numpy / scipy
+   fields to about 1e-14 relative. */
+int nls_field2d(int32_t kind, int32_t n, double L, const double *params, int32_t nparams, const double *in,
+                int32_t nin, double *out);
 /* Free the slot (waits for its outstanding snapshot copies). */
 int nls_pool_release(nls_pool *pool, int32_t slot);
 /* Wait for all queued device work and copies. */

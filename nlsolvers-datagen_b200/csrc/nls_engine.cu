@@ -20,6 +20,7 @@
 #include "nls_kernels.cuh"
 #include "nls_downsample.cuh"
 #include "nls_fft_downsample.cuh"
+#include "nls_fields.cuh"
 
 using namespace nlsb;
 
@@ -1812,6 +1813,164 @@ int nls_downsample_fft(int32_t dim, const int64_t *shape, const int64_t *target,
   for (int f = 0; f < frames && e == cudaSuccess; ++f)
     e = fft_ds_field(plan, din + (int64_t)f * src, !is_complex, dout + (int64_t)f * dst, !is_complex, nullptr);
   if (e == cudaSuccess) e = cudaMemcpy(out, dout, out_b, cudaMemcpyDeviceToHost);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
+  return NLS_OK;
+}
+
+namespace {
+// Parameter count nls_field2d needs for `kind` (-1: malformed), the number of
+// input fields, and for the filtered kinds the offsets of the filters' taps.
+int64_t field_param_count(int kind, const double *P, int64_t np, int &need_in, std::vector<int64_t> &filt) {
+  need_in = 0;
+  filt.clear();
+  auto at = [&](int64_t i) -> double { return i < np ? P[i] : -1.0; };
+  auto cnt = [&](int64_t i) -> int64_t {
+    const double v = at(i);
+    return (v >= 0 && v <= (1 << 20) && v == (double)(int64_t)v) ? (int64_t)v : -1;
+  };
+  switch (kind) {
+    case FLD_M_PIECEWISE: return 5;
+    case FLD_M_GRADIENT: need_in = 1; return 3;
+    case FLD_M_PHASE: need_in = 1; return 3;
+    case FLD_M_TOPOLOGICAL: {
+      need_in = 1;
+      const int64_t t = cnt(3);
+      if (t < 1 || t % 2 == 0) return -1;
+      filt.push_back(3);
+      return 4 + t;
+    }
+    case FLD_M_DEFECTS: { const int64_t q = cnt(1); return q < 0 ? -1 : 2 + 4 * q; }
+    case FLD_M_QUASIPERIODIC:
+    case FLD_C_QUASIPERIODIC: { const int64_t q = cnt(1); return q < 0 ? -1 : 2 + 4 * q; }
+    case FLD_C_PERIODIC: return 3;
+    case FLD_C_PIECEWISE: return cnt(0) < 0 ? -1 : 4;
+    case FLD_C_SIGN: return 4;
+    case FLD_C_LAYERED: { const int64_t q = cnt(1); return q < 0 ? -1 : 2 + 5 * q; }
+    case FLD_C_WAVEGUIDE: {
+      const int64_t g = cnt(2), pts = cnt(3);
+      if (g < 0 || pts < 1) return -1;
+      return 4 + g * (1 + 2 * pts);
+    }
+    case FLD_M_MULTISCALE:
+    case FLD_C_TURBULENT: {
+      const int64_t q = cnt(kind == FLD_M_MULTISCALE ? 1 : 2);
+      if (q < 0) return -1;
+      need_in = (int)q;
+      int64_t o = kind == FLD_M_MULTISCALE ? 2 : 3;
+      for (int64_t i = 0; i < q; ++i) {
+        const int64_t t = cnt(o + 1);
+        if (t < 1 || t % 2 == 0) return -1;
+        filt.push_back(o + 1);
+        o += 2 + t;
+      }
+      return o;
+    }
+    default: return -1;
+  }
+}
+}  // namespace
+
+int nls_field2d(int32_t kind, int32_t n, double L, const double *params, int32_t nparams, const double *in,
+                int32_t nin, double *out) {
+  if (!out || n < 2 || n > (1 << 15) || nparams < 0 || (nparams && !params) || nin < 0 || (nin && !in))
+    return fail(NLS_ERR_INVALID_ARG, "bad field arguments");
+  int need_in = 0;
+  std::vector<int64_t> filt;
+  const int64_t need = field_param_count(kind, params, nparams, need_in, filt);
+  if (need < 0) return fail(NLS_ERR_INVALID_ARG, "unknown field kind or malformed parameter list");
+  if (need != nparams)
+    return fail(NLS_ERR_INVALID_ARG, "field kind " + std::to_string(kind) + " takes " + std::to_string(need) +
+                                         " parameters, got " + std::to_string(nparams));
+  if (nin != need_in)
+    return fail(NLS_ERR_INVALID_ARG, "field kind " + std::to_string(kind) + " takes " + std::to_string(need_in) +
+                                         " input fields, got " + std::to_string(nin));
+  const int64_t N = (int64_t)n * n;
+  const std::vector<double> x = np_linspace(L, n);
+  const size_t nb = sizeof(double) * (size_t)N;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t total = up(sizeof(double) * n) + up(sizeof(double) * std::max(nparams, 1)) +
+                       up(sizeof(double) * (3 + 3 * FLD_RED_BLOCKS)) + up(sizeof(int) * 4) +
+                       (nin ? up(nb * nin) : 0) + 3 * up(nb);
+  char *dev = nullptr;
+  CK(cudaMalloc((void **)&dev, total));
+  char *q = dev;
+  auto take = [&](size_t b) { char *r = q; q += up(b); return r; };
+  double *dx = (double *)take(sizeof(double) * n), *dP = (double *)take(sizeof(double) * std::max(nparams, 1));
+  double *dred = (double *)take(sizeof(double) * (3 + 3 * FLD_RED_BLOCKS));
+  double *dpart = dred + 3;
+  int *dtick = (int *)take(sizeof(int) * 4);
+  double *din = nin ? (double *)take(nb * nin) : nullptr;
+  double *dout = (double *)take(nb), *t0 = (double *)take(nb), *t1 = (double *)take(nb);
+  cudaError_t e = cudaMemcpy(dx, x.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nparams) e = cudaMemcpy(dP, params, sizeof(double) * nparams, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nin) e = cudaMemcpy(din, in, nb * nin, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dtick, 0, sizeof(int) * 4);
+  const int blocks = (int)std::min<int64_t>((N + 255) / 256, 4096);
+  auto point = [&](double *dst, const double *src) {
+    k_field_point<<<blocks, 256>>>(kind, n, L, dP, dx, src, dst);
+  };
+  auto reduce = [&](const double *v) { k_field_reduce<<<FLD_RED_BLOCKS, 256>>>(v, N, dpart, dtick, dred); };
+  auto op = [&](int o, const double *v, double *dst, double a, double base) {
+    k_field_op<<<blocks, 256>>>(o, v, dst, N, a, base, dred);
+  };
+  // gaussian_filter of src into dst (axis 0 into t1, then axis 1), taps at P[toff + 1 ..]
+  auto gauss = [&](const double *src, double *dst, int64_t toff) {
+    const int taps = (int)params[toff];
+    k_field_corr<<<blocks, 256>>>(src, t1, n, 0, dP + toff + 1, taps);
+    k_field_corr<<<blocks, 256>>>(t1, dst, n, 1, dP + toff + 1, taps);
+  };
+  if (e == cudaSuccess) {
+    switch (kind) {
+      case FLD_M_PHASE:  // m0 (1 + delta |grad| / max |grad|)
+        point(t0, din);
+        reduce(t0);
+        op(FOP_SCALE_NORM, t0, dout, params[1], params[0]);
+        break;
+      case FLD_M_TOPOLOGICAL:  // m0 (1 + eta G(sign(lap c - lambda c)) / max |.|)
+        k_field_topo<<<blocks, 256>>>(din, t0, n, params[2]);
+        gauss(t0, t0, filt[0]);
+        reduce(t0);
+        op(FOP_SCALE_NORM, t0, dout, params[1], params[0]);
+        break;
+      case FLD_C_QUASIPERIODIC:
+      case FLD_C_LAYERED:  // base (p - min) / (max - min)
+        point(t0, nullptr);
+        reduce(t0);
+        op(FOP_MINMAX, t0, dout, 0.0, params[0]);
+        break;
+      case FLD_M_MULTISCALE: {  // m0 + sum_s a_s G_s(noise_s) / max |.|, floored at 0.1 m0
+        op(FOP_FILL, nullptr, dout, params[0], 0.0);
+        int64_t o = 2;
+        for (int i = 0; i < need_in; ++i) {
+          gauss(din + (size_t)i * N, t0, o + 1);
+          reduce(t0);
+          op(FOP_ACC_NORM, t0, dout, params[o], 0.0);
+          o += 2 + (int64_t)params[o + 1];
+        }
+        op(FOP_FLOOR, dout, dout, 0.1 * params[0], 0.0);
+        break;
+      }
+      case FLD_C_TURBULENT: {  // f = sum_o a_o G_o(noise_o); base exp(intensity ((f - min) / max - 0.5))
+        op(FOP_FILL, nullptr, dout, 0.0, 0.0);
+        int64_t o = 3;
+        for (int i = 0; i < need_in; ++i) {
+          gauss(din + (size_t)i * N, t0, o + 1);
+          op(FOP_ACC, t0, dout, params[o], 0.0);
+          o += 2 + (int64_t)params[o + 1];
+        }
+        reduce(dout);
+        op(FOP_SUBMIN, dout, t0, 0.0, 0.0);
+        reduce(t0);
+        op(FOP_TURBEXP, t0, dout, params[1], params[0]);
+        break;
+      }
+      default:
+        point(dout, din);
+    }
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, nb, cudaMemcpyDeviceToHost);
   cudaFree(dev);
   if (e != cudaSuccess) return fail(NLS_ERR_CUDA, cudaGetErrorString(e));
   return NLS_OK;

@@ -37,6 +37,7 @@ SYMBOLS = [
     "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
     "nls_pool_set_downsample", "nls_downsample_linear", "nls_pool_snapshots_ready",
     "nls_pool_set_downsample_fft", "nls_downsample_fft", "nls_pool_set_step_kernel", "nls_pool_set_wait_limit",
+    "nls_field2d",
 ]
 
 
@@ -119,6 +120,7 @@ def lib() -> ctypes.CDLL:
         "nls_downsample_fft": [i32, ctypes.POINTER(i64), ctypes.POINTER(i64), i32, i32, dp, dp],
         "nls_pool_set_step_kernel": [vp, i32],
         "nls_pool_set_wait_limit": [vp, i64, i32],
+        "nls_field2d": [i32, i32, ctypes.c_double, dp, i32, dp, i32, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
