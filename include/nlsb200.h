@@ -251,6 +251,14 @@ int nls_pool_set_final_segment(nls_pool *pool, int32_t rows);
    with CUDA events; *ms = mean duration of one launch; *points = grid points
    covered by one launch. The pass is idempotent, so the state is unchanged. */
 int nls_pool_time_pass(nls_pool *pool, int32_t j, int32_t iters, float *ms, int64_t *points);
+/* Time the Lanczos passes j0..j1 (1 <= j0 <= j1 <= k-2) in the step's order,
+   `reps` times, launched back to back on each slot group's stream as the step
+   issues them (one fork before and one join after the whole sequence, so
+   consecutive passes overlap their launch as inside the step): *ms = mean
+   duration of one pass launch; *points = grid points covered by one launch.
+   nls_pool_time_pass instead forks and joins the groups around every launch,
+   which times a launch in isolation. */
+int nls_pool_time_passes(nls_pool *pool, int32_t j0, int32_t j1, int32_t reps, float *ms, int64_t *points);
 /* Advance like nls_pool_step and time the steps with CUDA events recorded on
    the pool's stream around them (waits for completion): *ms = device time of
    all nsteps steps. */

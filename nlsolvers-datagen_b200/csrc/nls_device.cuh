@@ -166,15 +166,20 @@ __device__ __forceinline__ void cp_async(void *smem, const void *gmem, int bytes
   else
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
-// Programmatic dependent launch: allow the next kernel of the stream to place
-// its blocks while this grid drains, then wait until the previous grid has
-// completed and its writes are visible. Called first in every step kernel that
-// the engine launches with the attribute, so nothing an earlier kernel wrote is
-// touched before the wait; without the attribute both are no-ops.
-__device__ __forceinline__ void pdl_entry() {
-  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+// Programmatic dependent launch. pdl_gate() waits until the previous grid of
+// the stream has completed and its writes are visible, and only then allows
+// the next kernel to place its blocks while this grid drains. Because every
+// step kernel releases its dependent only after its own wait, a kernel that
+// starts running finds the grid two launches back complete: data written two
+// or more kernels earlier (Krylov vectors of earlier passes, the fields of the
+// previous step) may be read before the gate, anything the immediately
+// preceding kernel writes only after it. pdl_entry() is the gate at kernel
+// entry. Without the launch attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_gate() {
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
+__device__ __forceinline__ void pdl_entry() { pdl_gate(); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));

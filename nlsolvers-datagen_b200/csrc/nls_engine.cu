@@ -2092,25 +2092,29 @@ int nls_pool_kernels_per_step(nls_pool *P, int32_t *count) {
   return NLS_OK;
 }
 
-int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t *points) {
-  if (!P || !ms || iters <= 0) return fail(NLS_ERR_INVALID_ARG, "null");
-  if (!is_krylov(P->method) || j < 1 || j > P->k - 2) return fail(NLS_ERR_INVALID_ARG, "bad pass index");
+// Pass timing. chain == false: every launch of pass j0 is forked onto the
+// groups' streams and joined again (a launch in isolation). chain == true:
+// passes j0..j1 in the step's order, reps times, launched back to back on each
+// group's stream with one fork before and one join after, so consecutive passes
+// follow each other as they do inside the step (programmatic dependent launch
+// between them). Every pass is idempotent on the current state.
+static int time_passes(nls_pool *P, int32_t j0, int32_t j1, int32_t reps, bool chain, float *ms, int64_t *points) {
+  if (!P || !ms || reps <= 0) return fail(NLS_ERR_INVALID_ARG, "null");
+  if (!is_krylov(P->method) || j0 < 1 || j1 < j0 || j1 > P->k - 2) return fail(NLS_ERR_INVALID_ARG, "bad pass index");
   if (P->tables_dirty) {
     int rc = rebuild_tables(P);
     if (rc) return rc;
   }
   if (P->main.nlist == 0) return fail(NLS_ERR_STATE, "no active slot");
   const Launch &L = P->cplx ? (P->method == NLS_NLSE_SS2 ? P->ks.ss2 : P->ks.sewi_a) : P->ks.kg;
-  // pass j over every main-step group, launched as the step launches it (the
-  // two groups side by side on the pool stream and stream2)
   StepArgs args[2];
   int grids[2];
-  LaunchFn fns[2];
+  LaunchFn fns[2], fns_lo[2];
   const int ng = P->split ? 2 : 1;
+  const int hc = P->step_hc;
   for (int g = 0; g < ng; ++g) {
     const TileSet &T = g ? P->main2 : P->main;
     StepArgs a = base_args(P, T, g);
-    a.j = j;
     a.op_sign = P->cplx ? 1.0 : -1.0;
     a.nseq = P->method == NLS_NLSE_SS2 ? 1 : 2;
     int grid = T.cap;
@@ -2118,27 +2122,56 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
     args[g] = a;
     grids[g] = grid;
     fns[g] = lf;
+    fns_lo[g] = (lf == L.lanczos[hc] && L.lanczos_lo[hc]) ? L.lanczos_lo[hc] : lf;
+  }
+  auto launch = [&](int g, int j, cudaStream_t st) -> cudaError_t {
+    StepArgs a = args[g];
+    a.j = j;
+    return (j == 1 ? fns_lo[g] : fns[g])(a, grids[g], st);
+  };
+  auto fork = [&]() -> int {
+    if (ng == 2) {
+      CK(cudaEventRecord(P->ev_fork, P->stream));
+      CK(cudaStreamWaitEvent(P->stream2, P->ev_fork, 0));
+    }
+    return NLS_OK;
+  };
+  auto join = [&]() -> int {
+    if (ng == 2) {
+      CK(cudaEventRecord(P->ev_join, P->stream2));
+      CK(cudaStreamWaitEvent(P->stream, P->ev_join, 0));
+    }
+    return NLS_OK;
+  };
+  auto run = [&]() -> int {
+    int rc = NLS_OK;
+    if (chain) {
+      if ((rc = fork())) return rc;
+      for (int r = 0; r < reps; ++r)
+        for (int j = j0; j <= j1; ++j)
+          for (int g = 0; g < ng; ++g) CK(launch(g, j, g ? P->stream2 : P->stream));
+      return join();
+    }
+    for (int r = 0; r < reps; ++r) {
+      if ((rc = fork())) return rc;
+      for (int g = 0; g < ng; ++g) CK(launch(g, j0, g ? P->stream2 : P->stream));
+      if ((rc = join())) return rc;
+    }
+    return NLS_OK;
+  };
+  // warm-up: one launch of every timed pass
+  {
+    int rc = fork();
+    for (int j = j0; j <= j1 && !rc; ++j)
+      for (int g = 0; g < ng; ++g) CK(launch(g, j, g ? P->stream2 : P->stream));
+    if (!rc) rc = join();
+    if (rc) return rc;
   }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  auto once = [&]() -> int {
-    if (ng == 1) {
-      CK(fns[0](args[0], grids[0], P->stream));
-      return NLS_OK;
-    }
-    CK(cudaEventRecord(P->ev_fork, P->stream));
-    CK(cudaStreamWaitEvent(P->stream2, P->ev_fork, 0));
-    CK(fns[0](args[0], grids[0], P->stream));
-    CK(fns[1](args[1], grids[1], P->stream2));
-    CK(cudaEventRecord(P->ev_join, P->stream2));
-    CK(cudaStreamWaitEvent(P->stream, P->ev_join, 0));
-    return NLS_OK;
-  };
-  int rc = once();  // warm
-  if (rc) return rc;
   CK(cudaEventRecord(e0, P->stream));
-  for (int i = 0; i < iters && !rc; ++i) rc = once();
+  int rc = run();
   if (rc) return rc;
   CK(cudaEventRecord(e1, P->stream));
   CK(cudaEventSynchronize(e1));
@@ -2146,7 +2179,7 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
   CK(cudaEventElapsedTime(&t, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  *ms = t / iters;
+  *ms = t / (float)((int64_t)reps * (chain ? (j1 - j0 + 1) : 1));
   if (points) {
     int64_t pts = 0;
     for (int s : P->main.list) pts += P->hs[s].n;
@@ -2154,6 +2187,14 @@ int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t
     *points = pts;
   }
   return NLS_OK;
+}
+
+int nls_pool_time_pass(nls_pool *P, int32_t j, int32_t iters, float *ms, int64_t *points) {
+  return time_passes(P, j, j, iters, false, ms, points);
+}
+
+int nls_pool_time_passes(nls_pool *P, int32_t j0, int32_t j1, int32_t reps, float *ms, int64_t *points) {
+  return time_passes(P, j0, j1, reps, true, ms, points);
 }
 
 int nls_pool_destroy(nls_pool *P) {

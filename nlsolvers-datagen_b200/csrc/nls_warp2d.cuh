@@ -808,32 +808,22 @@ __device__ __forceinline__ void final2_body(const StepArgs &a, const TileDesc *t
   using FR = FinRow<FIN, E>;
   constexpr int NB = 8;
   const int lane = threadIdx.x & 31;
-  if (wt >= ntiles) return;
+  if (wt >= ntiles) {
+    if (!DYN) pdl_gate();
+    return;
+  }
+  // Before the programmatic-launch gate: the tables and the first rows of
+  // V_{k-1} (written by the last pass, two kernels earlier). After it: the f(T)
+  // coefficients that the preceding kernel wrote, and the rows of the march.
   const TileDesc t = tiles[wt];
   const SlotDesc &s = a.slots[t.slot];
   const Strip S = make_strip<V16<E>::N>(s, t, lane);
-  const int step = a.state[t.slot].step;
   const int kv = a.kv;
   const R opsc = R(a.op_sign * s.inv_h2);
   const R *cf = (const R *)a.f.c;
   const E *VL[NSEQ];
-  R lr[NSEQ], li[NSEQ];
 #pragma unroll
-  for (int sq = 0; sq < NSEQ; ++sq) {
-    const FinalCoef &F = a.coef[t.slot * 2 + sq];
-    VL[sq] = (const E *)a.V + (long long)(sq * kv + kv - 1) * a.vstride;
-    if constexpr (sizeof(R) == 4) {
-      lr[sq] = F.lam32[0];
-      li[sq] = F.lam32[1];
-    } else {
-      lr[sq] = R(F.lam_r);
-      li[sq] = R(F.lam_i);
-    }
-    // lanes >= kv store zeros: the batched loop reads up to NB entries past kv-2
-    W[sq][lane][0] = lane < kv ? coef_w<R>(F, lane, false) : R(0);
-    W[sq][lane][1] = lane < kv ? coef_w<R>(F, lane, true) : R(0);
-  }
-  __syncwarp();
+  for (int sq = 0; sq < NSEQ; ++sq) VL[sq] = (const E *)a.V + (long long)(sq * kv + kv - 1) * a.vstride;
   const bool io = S.out_lane;
   V16<E> Lm[NSEQ], Lo[NSEQ], Lp[NSEQ], Ln1[NSEQ];
   CRow<E> cw[3], cn1;
@@ -849,6 +839,24 @@ __device__ __forceinline__ void final2_body(const StepArgs &a, const TileDesc *t
     cw[2] = load_crow<E>(cf, S, r0);
     cn1 = load_crow<E>(cf, S, r0 + 1);
   }
+  if (!DYN) pdl_gate();
+  const int step = a.state[t.slot].step;
+  R lr[NSEQ], li[NSEQ];
+#pragma unroll
+  for (int sq = 0; sq < NSEQ; ++sq) {
+    const FinalCoef &F = a.coef[t.slot * 2 + sq];
+    if constexpr (sizeof(R) == 4) {
+      lr[sq] = F.lam32[0];
+      li[sq] = F.lam32[1];
+    } else {
+      lr[sq] = R(F.lam_r);
+      li[sq] = R(F.lam_i);
+    }
+    // lanes >= kv store zeros: the batched loop reads up to NB entries past kv-2
+    W[sq][lane][0] = lane < kv ? coef_w<R>(F, lane, false) : R(0);
+    W[sq][lane][1] = lane < kv ? coef_w<R>(F, lane, true) : R(0);
+  }
+  __syncwarp();
   for (int r = r0; r < r1; ++r) {
     // ---- issue the row's loads
     V16<E> Ln2[NSEQ];
@@ -924,7 +932,7 @@ __device__ __forceinline__ void final2_body(const StepArgs &a, const TileDesc *t
 
 template <typename E, int NSEQ, int FIN, bool HC>
 __global__ void __launch_bounds__(32 * WPB, std::is_same<E, float>::value ? 4 : 1) k2_final(StepArgs a) {
-  pdl_entry();
+  // the programmatic-launch gate is inside the body, after the first rows' loads
   using R = typename Traits<E>::R;
   __shared__ R Wsh[WPB][NSEQ][KMAX][2];
   final2_body<E, NSEQ, FIN, HC, false>(a, a.tiles, *a.ntiles, blockIdx.x * WPB + (threadIdx.x >> 5),
@@ -1401,22 +1409,36 @@ __device__ __forceinline__ F4 lds16(uint32_t saddr) {
 // Lanczos matrix (T[k-1,k-1] = 0) makes the result sensitive to the
 // high-frequency rounding noise of the start vector under the stencil; later
 // vectors can be rounded to FP32 without effect.
-template <bool EDGE, bool LO = false>
+// The march's prologue copies the first CPD rows of ring B (V_{j-2}, written
+// two or more kernels earlier) as one commit group, then calls gate() (the
+// programmatic-launch wait, and the coefficients CA, CB, CSx, which come from
+// the previous pass), then copies the first CPD rows of ring A (V_{j-1}) one
+// group per row; from there one group per fetch holds A and B row r0-2+f.
+template <bool EDGE, bool LO = false, typename Gate>
 __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB, const float *safe, float *pJ, int P,
-                                                int r0, int r1, int ny, bool ld, bool io, bool hasB, float2 CA,
-                                                float2 CB, const F4 &CSx, const F4 &OPx, const F4 &xmiss,
-                                                double *acc, uint32_t cellA, uint32_t cellB, bool lo = false) {
+                                                int r0, int r1, int ny, bool ld, bool io, bool hasB, const float2 &CA,
+                                                const float2 &CB, const F4 &CSx, const F4 &OPx, const F4 &xmiss,
+                                                double *acc, uint32_t cellA, uint32_t cellB, bool lo, Gate &&gate) {
   const bool bl = LO && lo;  // ring B carries the low word of V_0
   // fetch f: A row r0-2+f into slot f % CPD of ring A, B row r0-2+f into ring B
-  // (fetch 0 of B is never read); one commit group per fetch
-  auto fetch = [&](int f) {
+  // (fetch 0 of B is never read)
+  auto fetchA = [&](int f) {
+    const int r = r0 - 2 + f;
+    const uint32_t off = (uint32_t)((f % CPD) * 512);
+    const bool okA = EDGE ? (ld && r >= 0 && r < ny && r <= r1 + 1) : (ld && r <= r1 + 1);
+    cp16z(cellA + off, okA ? (const void *)(pA + r * P) : (const void *)safe, okA);
+  };
+  auto fetchB = [&](int f) {
     const int r = r0 - 2 + f;
     const uint32_t off = (uint32_t)((f % CPD) * 512);
     const bool okA = EDGE ? (ld && r >= 0 && r < ny && r <= r1 + 1) : (ld && r <= r1 + 1);
     const bool okB = bl ? okA
                         : EDGE ? (ld && hasB && f >= 1 && r >= 0 && r < ny && r <= r1) : (ld && hasB && f >= 1 && r <= r1);
-    cp16z(cellA + off, okA ? (const void *)(pA + r * P) : (const void *)safe, okA);
     cp16z(cellB + off, okB ? (const void *)(pB + r * P) : (const void *)safe, okB);
+  };
+  auto fetch = [&](int f) {
+    fetchA(f);
+    fetchB(f);
     cp_async_commit();
   };
   // interior segments: each lane's row pointers advance by the pitch per
@@ -1439,11 +1461,24 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
     soff = (soff + 512) & RM;
     cp_async_commit();
   };
+  // prologue: ring B, the gate, ring A (fetches 0 .. CPD-1)
 #pragma unroll
   for (int f = 0; f < CPD; ++f) {
-    if (EDGE) fetch(f);
-    else fetch_fast(f);
+    if (EDGE) fetchB(f);
+    else if (f >= fB_first && f <= fB_last) cp16s(cellB + f * 512, gB + f * stB, szB);
   }
+  cp_async_commit();
+  gate();
+#pragma unroll
+  for (int f = 0; f < CPD; ++f) {
+    if (EDGE) fetchA(f);
+    else if (f <= fA_last) cp16s(cellA + f * 512, gA + f * stA, szA);
+    cp_async_commit();
+  }
+  gA += CPD * stA;
+  gB += CPD * stB;
+  // CPD + 1 groups issued; waiting for all but the newest CPD - 2 completes
+  // ring B's group and A rows 0, 1
   cp_async_wait<CPD - 2>();
   F4 A0 = lds16(cellA), A1 = lds16(cellA + 512), A2;
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
@@ -1555,18 +1590,17 @@ __device__ __forceinline__ void lz_f32c_body(const StepArgs &a, const TileDesc *
                                              int j, int wt, uint32_t cellA, uint32_t cellB, int *done) {
   using E = float;
   const int lane = threadIdx.x & 31;
-  if (wt >= ntiles) return;
+  if (wt >= ntiles) {
+    if (!DYN) pdl_gate();
+    return;
+  }
+  // before the gate: the tile tables, the slot's geometry and ring B's rows
+  // (written two or more kernels earlier); the previous pass's scalars after it
   const TileDesc t = tiles[wt];
   const SlotDesc &s = a.slots[t.slot];
   const Strip S = make_strip<V16<E>::N>(s, t, lane);
   const int sq = t.local & 1;
   const float opsc = float(a.op_sign * s.inv_h2);
-  const LzScal L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
-  const double b0 = a.beta0[t.slot * 2 + sq];
-  const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
-  const double sA = j == 1 ? s0 : 1.0, sB = j == 2 ? s0 : 1.0;
-  const float cs = float(sA * L.inv_b) * opsc;
-  const float2 CA = f2(float(-L.ar * sA * L.inv_b)), CB = f2(float(-L.dr * sB * L.inv_b));
   const long long vo = (long long)sq * a.kv;
   const bool hasB = j >= 2;
   const float *base = (const float *)a.V + (vo + j - 1) * a.vstride + s.off;
@@ -1580,7 +1614,7 @@ __device__ __forceinline__ void lz_f32c_body(const StepArgs &a, const TileDesc *
                     : u0B ? (const float *)a.f.u_hi + lane_off
                           : (const float *)a.V + (vo + (hasB ? j - 2 : 0)) * a.vstride + lane_off;
   float *pJ = (float *)a.V + (vo + j) * a.vstride + lane_off;
-  F4 CSx, OPx, xmiss;
+  F4 VMx, OPx, xmiss;
   {
     float v[4], m[4];
 #pragma unroll
@@ -1589,19 +1623,36 @@ __device__ __forceinline__ void lz_f32c_body(const StepArgs &a, const TileDesc *
       v[e] = (x >= 0 && x < S.nx) ? 1.f : 0.f;
       m[e] = float((x == 0) + (x == S.nx - 1));
     }
-    CSx = F4{make_float2(v[0] * cs, v[1] * cs), make_float2(v[2] * cs, v[3] * cs)};
+    VMx = F4{make_float2(v[0], v[1]), make_float2(v[2], v[3])};
     OPx = F4{make_float2(v[0] * opsc, v[1] * opsc), make_float2(v[2] * opsc, v[3] * opsc)};
     xmiss = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
   }
+  LzScal L;
+  double sA = 1.0;
+  float2 CA, CB;
+  F4 CSx;
+  auto gate = [&]() {
+    if (!DYN) pdl_gate();
+    L = a.scal[(t.slot * 2 + sq) * KMAX + (j - 1)];
+    const double b0 = a.beta0[t.slot * 2 + sq];
+    const double s0 = b0 > 0.0 ? 1.0 / b0 : 0.0;
+    sA = j == 1 ? s0 : 1.0;
+    const double sB = j == 2 ? s0 : 1.0;
+    const float cs = float(sA * L.inv_b) * opsc;
+    CA = f2(float(-L.ar * sA * L.inv_b));
+    CB = f2(float(-L.dr * sB * L.inv_b));
+    const float2 c2 = f2(cs);
+    CSx = F4{mul2(VMx.a, c2), mul2(VMx.b, c2)};
+  };
   const bool ld = S.lane_in, io = S.out_lane;
   const int r0 = t.p0, r1 = t.p1, ny = S.ny, P = s.pitch;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   if (r0 >= 2 && r1 <= ny - 2)
     lz1f32_cp_march<false, LO>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA,
-                               cellB, lo);
+                               cellB, lo, gate);
   else
     lz1f32_cp_march<true, LO>(pA, pB, base, pJ, P, r0, r1, ny, ld, io, hasB, CA, CB, CSx, OPx, xmiss, acc, cellA,
-                              cellB, lo);
+                              cellB, lo, gate);
   acc[0] *= sA;
   acc[2] *= sA;
   constexpr int ND = 6;
@@ -1628,7 +1679,7 @@ __device__ __forceinline__ void lz_f32c_body(const StepArgs &a, const TileDesc *
 
 template <int MINB, bool LO = false>
 __global__ void __launch_bounds__(32 * WPB, MINB) k2_lanczos1_f32c(StepArgs a) {
-  pdl_entry();
+  // the programmatic-launch gate is inside the body, after ring B's first rows
   __shared__ __align__(16) unsigned char ring[WPB][2][CPD][512];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   lz_f32c_body<LO, false>(a, a.tiles, *a.ntiles, *a.lt_stride, a.j, blockIdx.x * WPB + wib,
@@ -1656,11 +1707,14 @@ __device__ __forceinline__ F4 f4_force(int kind, const F4 &u, const F4 &m, const
             make_float2(kg_force<float>(kind, u.b.x, m.b.x, s), kg_force<float>(kind, u.b.y, m.b.y, s))};
 }
 
-template <bool EDGE, int SQ>
+// The first six raw rows (u, and m for sequence 1) are loaded before gate()
+// (the programmatic-launch wait, which also sets `step`, written by the
+// preceding kernel); the source rows are formed after it.
+template <bool EDGE, int SQ, typename Gate>
 __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM, float *pV, int P, int r0, int r1,
                                                 int ny, bool ld, bool io, const SlotDesc &s, const Strip &S,
-                                                int step, const F4 &OPx, const F4 &xmiss, double *acc,
-                                                bool store = true) {
+                                                const int &step, const F4 &OPx, const F4 &xmiss, double *acc,
+                                                bool store, Gate &&gate) {
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
   const float2 P1 = f2(float(s.p1)), Q1 = f2(float(s.q1)), P3 = f2(float(s.p3)), Q3 = f2(float(s.q3));
   const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
@@ -1692,10 +1746,12 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
     return x;
   };
   float2 q1 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
-  // x rows r0-1, r0 made; raw rows r0+1 .. r0+4 in flight
-  F4 X0 = make(rowU(r0 - 1), rowM(r0 - 1), r0 - 1), X1 = make(rowU(r0), rowM(r0), r0), X2 = zero4, X3 = zero4;
+  // raw rows r0-1 .. r0+4 in flight; x rows r0-1, r0 made after the gate
+  const F4 Ua = rowU(r0 - 1), Ma = rowM(r0 - 1), Ub = rowU(r0), Mb = rowM(r0);
   F4 U0 = rowU(r0 + 1), U1 = rowU(r0 + 2), U2 = rowU(r0 + 3), U3 = rowU(r0 + 4);
   F4 M0 = rowM(r0 + 1), M1 = rowM(r0 + 2), M2 = rowM(r0 + 3), M3 = rowM(r0 + 4);
+  gate();
+  F4 X0 = make(Ua, Ma, r0 - 1), X1 = make(Ub, Mb, r0), X2 = zero4, X3 = zero4;
   const int nit = (r1 - r0 + 3) / 4 * 4;
 #define NLSB_FIRST(Xm, Xc, Xp, Uc, Mc)                                                     \
   {                                                                                        \
@@ -1741,11 +1797,18 @@ __device__ __forceinline__ void first_f32_body(const StepArgs &a, const TileDesc
                                                int wt, int *done) {
   using E = float;
   const int lane = threadIdx.x & 31;
-  if (wt >= ntiles) return;
+  if (wt >= ntiles) {
+    if (!DYN) pdl_gate();
+    return;
+  }
   const TileDesc t = tiles[wt];
   const SlotDesc &s = a.slots[t.slot];
   const Strip S = make_strip<V16<E>::N>(s, t, lane);
-  const int step = a.state[t.slot].step;
+  int step = 0;  // the step counter is written by the preceding kernel (k_advance)
+  auto gate = [&]() {
+    if (!DYN) pdl_gate();
+    step = a.state[t.slot].step;
+  };
   const int sq = t.local & 1;
   const float opsc = float(a.op_sign * s.inv_h2);
   F4 OPx, xmiss;
@@ -1771,11 +1834,11 @@ __device__ __forceinline__ void first_f32_body(const StepArgs &a, const TileDesc
   if (sq == 0) {
     // V_0 of the cosine sequence is u_hi itself: stored only when the passes read it from V
     const bool st = !a.v0_u;
-    if (inner) first_f32_march<false, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st);
-    else first_f32_march<true, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st);
+    if (inner) first_f32_march<false, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st, gate);
+    else first_f32_march<true, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st, gate);
   } else {
-    if (inner) first_f32_march<false, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
-    else first_f32_march<true, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc);
+    if (inner) first_f32_march<false, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, true, gate);
+    else first_f32_march<true, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, true, gate);
   }
   constexpr int ND = 6;
   double vals[ND];
@@ -1799,7 +1862,7 @@ __device__ __forceinline__ void first_f32_body(const StepArgs &a, const TileDesc
 }
 
 static __global__ void __launch_bounds__(32 * WPB) k2_first_f32(StepArgs a) {
-  pdl_entry();
+  // the programmatic-launch gate is inside the body, after the first rows' loads
   first_f32_body<false>(a, a.tiles, *a.ntiles, *a.lt_stride, blockIdx.x * WPB + (threadIdx.x >> 5), nullptr);
 }
 

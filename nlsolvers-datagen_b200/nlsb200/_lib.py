@@ -31,7 +31,7 @@ SYMBOLS = [
     "nls_problem_defaults", "nls_create", "nls_step", "nls_run", "nls_snapshot",
     "nls_steps_done", "nls_destroy", "nls_pool_create", "nls_pool_admit", "nls_pool_step",
     "nls_pool_poll", "nls_pool_release", "nls_pool_sync", "nls_pool_usage",
-    "nls_pool_set_graphs", "nls_pool_set_segment", "nls_pool_set_final_segment", "nls_pool_time_pass",
+    "nls_pool_set_graphs", "nls_pool_set_segment", "nls_pool_set_final_segment", "nls_pool_time_pass", "nls_pool_time_passes",
     "nls_pool_kernels_per_step", "nls_pool_destroy", "nls_strerror", "nls_last_error",
     "nls_pool_step_timed", "nls_set_device", "nls_host_alloc", "nls_host_free",
     "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
@@ -103,6 +103,7 @@ def lib() -> ctypes.CDLL:
         "nls_pool_set_segment": [vp, i32],
         "nls_pool_set_final_segment": [vp, i32],
         "nls_pool_time_pass": [vp, i32, i32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(i64)],
+        "nls_pool_time_passes": [vp, i32, i32, i32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(i64)],
         "nls_pool_kernels_per_step": [vp, ip],
         "nls_pool_step_timed": [vp, i32, ctypes.POINTER(ctypes.c_float)],
         "nls_pool_destroy": [vp],

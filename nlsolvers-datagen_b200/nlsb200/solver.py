@@ -401,6 +401,14 @@ class Pool:
         check(lib().nls_pool_time_pass(self._p, j, iters, ctypes.byref(ms), ctypes.byref(pts)))
         return ms.value, pts.value
 
+    def time_passes(self, j0: int, j1: int, reps: int):
+        """Mean duration (ms) of one Lanczos pass launch over passes j0..j1
+        launched back to back as the step issues them, and the grid points
+        one launch covers."""
+        ms, pts = ctypes.c_float(), ctypes.c_int64()
+        check(lib().nls_pool_time_passes(self._p, j0, j1, reps, ctypes.byref(ms), ctypes.byref(pts)))
+        return ms.value, pts.value
+
     def set_step_kernel(self, one_kernel: bool):
         """2-D FP32 Gautschi pools: run each step as one kernel (True) or as
         the launch sequence (False, the default); see nls_pool_set_step_kernel."""
