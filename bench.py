@@ -51,7 +51,7 @@ FALLBACK_HBM = 6650.0
 # DRAM bytes (read + write) per grid point of one Lanczos pass launch
 # (k2_lanczos1_f32c, j = 2, both sequences) in the ncu capture of
 # profiles/ncu_lanczos_pass_kg2d.md; algorithmic: 24 B per point.
-TRAFFIC_BYTES_PER_POINT_PASS = 17.94
+TRAFFIC_BYTES_PER_POINT_PASS = 17.79
 TIMED_REGION_S = 1.0
 
 
@@ -383,29 +383,111 @@ def run_reference(args, ws, rank, budget_s=150.0):
 
 
 SERVE_RATES_HZ = (2.0, 8.0, 32.0)
+SERVE_WINDOW_S = 4.0  # arrivals span about this long at each rate
+SERVE_REQUESTS = (12, 64)  # fewest and most requests of one rate's stream
 
 
-def serving_leg(count=24, rates=SERVE_RATES_HZ, steps=(500, 5000), seed=5, budget_gib=8.0):
+def _serve_once(serve, reqs, budget):
+    srv = serve.Server(serve.default_classes(reqs, max_slots=32), chunk=20, memory_budget=budget)
+    st = srv.run(reqs, timeout_s=600)
+    srv.close()
+    row = st.summary()
+    row.update({"requests": len(reqs), "classes": sorted({r.cls for r in reqs}), "gp_steps": st.gp_steps})
+    return row
+
+
+def serving_leg(rates=SERVE_RATES_HZ, window_s=SERVE_WINDOW_S, steps=(500, 5000), seed=5, budget_gib=8.0):
     """The serving mix (requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
     64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D, 500-5000 steps each, Poisson
     arrivals) at each rate of `rates`: latency percentiles (arrival to last
     snapshot on the host) and aggregate throughput (all requests' grid-point
-    steps over the run's wall time). Admission by an 8 GiB device-memory
-    budget shared by the class pools; page-locked client snapshot buffers."""
+    steps over the run's wall time). Each rate's stream holds rate x window_s
+    requests (at least 12, at most 64), so the highest rate keeps the server
+    loaded for most of its run. "saturated" serves the highest rate's requests
+    all arriving at once: the throughput ceiling of this mix on this server.
+    Admission by an 8 GiB device-memory budget shared by the class pools;
+    page-locked client snapshot buffers."""
     from nlsb200 import serve
-    out = {"rates": [], "requests_per_rate": count, "steps_per_request": list(steps), "unit": UNIT,
-           "memory_budget_bytes": int(budget_gib * (1 << 30)), "snapshots_per_request": 5}
+    budget = int(budget_gib * (1 << 30))
+    out = {"rates": [], "arrival_window_s": window_s, "steps_per_request": list(steps), "unit": UNIT,
+           "memory_budget_bytes": budget, "snapshots_per_request": 5}
+    reqs = None
     for i, rate in enumerate(rates):
+        count = int(min(max(round(rate * window_s), SERVE_REQUESTS[0]), SERVE_REQUESTS[1]))
         reqs = serve.mixed_requests(count, rate, seed=seed + i, steps=steps, ns=5, pinned=True)
-        srv = serve.Server(serve.default_classes(reqs, max_slots=32), chunk=20,
-                           memory_budget=int(budget_gib * (1 << 30)))
-        st = srv.run(reqs, timeout_s=600)
-        srv.close()
-        row = st.summary()
-        row.update({"rate_hz": rate, "classes": sorted({r.cls for r in reqs}),
-                    "gp_steps": st.gp_steps})
+        row = _serve_once(serve, reqs, budget)
+        row["rate_hz"] = rate
         out["rates"].append(row)
-        del reqs
+    for r in reqs:  # the last (highest) rate's requests, all at t = 0
+        r.arrival, r.t_admit, r.t_done, r.slot, r.traj = 0.0, float("nan"), float("nan"), -1, None
+    out["saturated"] = _serve_once(serve, reqs, budget)
+    del reqs
+    return out
+
+
+def other_configs_leg(steps=20, reps=3):
+    """The other batched configurations, timed the same way as the headline
+    (inputs resident, graph replay, CUDA events on the pool stream, median of
+    `reps` blocks of `steps` steps after 3 warm-up steps):
+      - NLSE 2-D SS2, 128 x 200^2 on [-10,10]^2, dt = 1e-3, k = 12, complex64;
+      - KG 3-D Gautschi, 40 x 220^3 on [-10,10]^3, dt = 0.01, k = 10, FP32.
+    The fields of NLSE trajectory i are those of seed i % 16, of 3-D
+    trajectory i those of seed i % 4 (the shapes and distributions of the
+    configuration; fewer distinct fields keep the host-side generation short).
+    Each entry carries the roofline of its Lanczos pass: 24 algorithmic bytes
+    per grid point (three vectors of 8 B for complex64 with one sequence, of
+    4 B for each of the two real sequences), passes j = 2..k-2 back to back."""
+    import nlsb200 as nl
+    from nlsb200 import workloads as W
+    from nlsb200.solver import FP32, KG_GAUTSCHI, NLSE_SS2, Pool
+    peak, peak_kind = hbm_peak()
+    out = {}
+    for name in ("nlse2d_200_b128", "kg3d_220_b40"):
+        cfg = W.CONFIGS[name]
+        n, B, k = cfg["n"], cfg["batch"], cfg["k"]
+        dim = 3 if name.startswith("kg3d") else 2
+        distinct = 16 if dim == 2 else 4
+        if dim == 2:
+            base = [W.nlse_case(n, cfg["L"], cfg["T"], cfg["nt"], cfg["ns"], k=k, seed=i, precision=FP32)
+                    for i in range(distinct)]
+            method = NLSE_SS2
+        else:
+            base = [W.kg_case(n, cfg["L"], cfg["T"], cfg["nt"], cfg["ns"], k=k, seed=i, dim=3, precision=FP32)
+                    for i in range(distinct)]
+            method = KG_GAUTSCHI
+        if dim == 3:
+            # one snapshot (the initial state): at the configuration's cadence
+            # (every 250 steps) the timed steps hold no snapshot step either
+            for sp, *_ in base:
+                sp.ns = 1
+        # every trajectory's host snapshot buffer is one shared page-locked array
+        # (the timing leg reads no result back)
+        sp0 = base[0][0]
+        shared_traj = nl.pinned_empty((sp0.ns,) + sp0.shape, np.complex128 if dim == 2 else np.float64)
+        shared_vel = None if dim == 2 else nl.pinned_empty((sp0.ns,) + sp0.shape)
+        cases = [base[i % distinct] for i in range(B)]
+        pts = ((n + 31) // 32 * 32) * n * (n if dim == 3 else 1)
+        # NLSE 2-D: 25-row pass segments, 12-row final tiles; 3-D: 88-plane segments (the default)
+        pool = Pool(method, dim, k, FP32, capacity_points=B * (pts + 256), max_slots=B,
+                    segment=25 if dim == 2 else None, final_segment=12 if dim == 2 else None)
+        for cs in cases:
+            assert pool.admit(*cs, traj=shared_traj, vel=shared_vel) is not None
+        pool.step(3)
+        pool.sync()
+        ms = statistics.median([pool.step_timed(steps) / steps for _ in range(reps)])
+        pass_ms, ppts = pool.time_passes(2, k - 2, 5)
+        pool.close()
+        npts = B * n ** dim
+        achieved = 24 * ppts / (pass_ms / 1e3) / 1e9
+        out[name] = {
+            "workload": (f"NLSE 2-D SS2, {B} x {n}^2 on [-10,10]^2, dt=1e-3, k={k}, complex64" if dim == 2 else
+                         f"KG 3-D Gautschi, {B} x {n}^3 on [-10,10]^3, dt=0.01, k={k}, FP32"),
+            "ms_per_step": ms, "value": npts / (ms / 1e3), "unit": UNIT, "steps": steps * reps,
+            "pass_roofline": {"kernel": "k2_lanczos1_c32" if dim == 2 else "k3_lanczos_f32",
+                              "launch_ms": pass_ms, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                              "frac": achieved / peak, "peak_kind": peak_kind},
+        }
+        del base, cases, shared_traj, shared_vel
     return out
 
 
@@ -590,6 +672,8 @@ def run_ours(args, ws, rank, lrank):
     }
     if ws == 1 and not args.no_serve:
         line["serving"] = serving_leg()
+    if ws == 1 and not args.no_other:
+        line["other_configs"] = other_configs_leg()
     if ws == 1 and rank == 0 and not args.no_cpu:
         line["cpu_baseline"], line["parity"] = cpu_parity_leg(k, traj0, vel0)
     if rank == 0:
@@ -618,6 +702,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline and parity leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-mix leg")
+    ap.add_argument("--no-other", action="store_true", help="skip the NLSE 2-D and KG 3-D batched configurations")
     ap.add_argument("--small", action="store_true",
                     help="profiling case of --batch trajectories (no autotune, e2e or CPU leg)")
     ap.add_argument("--batch", type=int, default=16, help="trajectories of the --small case")

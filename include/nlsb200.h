@@ -236,6 +236,15 @@ int nls_field2d(int32_t kind, int32_t n, double L, const double *params, int32_t
 int nls_pool_release(nls_pool *pool, int32_t slot);
 /* Wait for all queued device work and copies. */
 int nls_pool_sync(nls_pool *pool);
+/* Mark the device work queued on the pool so far (the steps and admissions,
+   not the snapshot copies) and return its ticket; nls_pool_fence_wait blocks
+   until the work before that mark has run, then reports the slots' device
+   status as nls_pool_sync does. Only the last 16 fences of a pool can be
+   waited on (NLS_ERR_INVALID_ARG otherwise). A host loop that keeps the next
+   chunk of steps queued while it waits for the previous one uses these in
+   place of nls_pool_sync. */
+int nls_pool_fence(nls_pool *pool, int32_t *ticket);
+int nls_pool_fence_wait(nls_pool *pool, int32_t ticket);
 /* Number of occupied slots, and free device points. */
 int nls_pool_usage(nls_pool *pool, int32_t *occupied, int64_t *free_points);
 /* 1: capture each step as a CUDA graph (default), 0: direct launches. */

@@ -497,6 +497,10 @@ struct nls_pool {
   int segf2 = 0;             // rows of the 2-D final pass's tiles (0: seg2)
   cudaStream_t stream = nullptr, copy_stream = nullptr, stream2 = nullptr;
   cudaEvent_t ev_step = nullptr, ev_fork = nullptr, ev_join = nullptr;
+  // nls_pool_fence: events recorded on the pool stream, a ring of NFENCE
+  static constexpr int NFENCE = 16;
+  cudaEvent_t fence_ev[NFENCE] = {};
+  int32_t fence_next = 0;
   bool use_graph = true;
   cudaGraphExec_t gexec = nullptr;
   int graph_tiles = -1, graph_ring = -1, graph_hc = -1;
@@ -2015,11 +2019,35 @@ int nls_set_diagnostics(nls_handle *H, double *diag_dst) {
   return nls_pool_set_diagnostics(H->pool, H->slot, diag_dst);
 }
 
+static int pool_status(nls_pool *P);
+
 int nls_pool_sync(nls_pool *P) {
   if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
   CK(cudaStreamSynchronize(P->stream));
   CK(cudaStreamSynchronize(P->copy_stream));
-  // device-side status (eigensolver convergence)
+  return pool_status(P);
+}
+
+int nls_pool_fence(nls_pool *P, int32_t *ticket) {
+  if (!P || !ticket) return fail(NLS_ERR_INVALID_ARG, "null");
+  const int i = P->fence_next % nls_pool::NFENCE;
+  if (!P->fence_ev[i]) CK(cudaEventCreateWithFlags(&P->fence_ev[i], cudaEventDisableTiming));
+  CK(cudaEventRecord(P->fence_ev[i], P->stream));
+  *ticket = P->fence_next++;
+  return NLS_OK;
+}
+
+int nls_pool_fence_wait(nls_pool *P, int32_t ticket) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  if (ticket < 0 || ticket >= P->fence_next || P->fence_next - ticket > nls_pool::NFENCE)
+    return fail(NLS_ERR_INVALID_ARG, "fence " + std::to_string(ticket) + " is not one of the last " +
+                                         std::to_string(nls_pool::NFENCE) + " fences of the pool");
+  CK(cudaEventSynchronize(P->fence_ev[ticket % nls_pool::NFENCE]));
+  return pool_status(P);
+}
+
+// device-side status of the slots (eigensolver convergence, divergence, waits)
+static int pool_status(nls_pool *P) {
   std::vector<SlotState> st(P->max_slots);
   CK(cudaMemcpy(st.data(), P->d_state, sizeof(SlotState) * P->max_slots, cudaMemcpyDeviceToHost));
   for (int s = 0; s < P->max_slots; ++s) {
@@ -2223,6 +2251,8 @@ int nls_pool_destroy(nls_pool *P) {
   cudaEventDestroy(P->ev_step);
   cudaEventDestroy(P->ev_fork);
   cudaEventDestroy(P->ev_join);
+  for (cudaEvent_t e : P->fence_ev)
+    if (e) cudaEventDestroy(e);
   delete P;
   return NLS_OK;
 }

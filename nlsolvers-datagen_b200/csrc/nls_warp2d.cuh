@@ -1465,18 +1465,18 @@ __device__ __forceinline__ void lz1f32_cp_march(const float *pA, const float *pB
 #pragma unroll
   for (int f = 0; f < CPD; ++f) {
     if (EDGE) fetchB(f);
-    else if (f >= fB_first && f <= fB_last) cp16s(cellB + f * 512, gB + f * stB, szB);
+    else if (f >= fB_first && f <= fB_last) cp16s(cellB + f * 512, gB, szB);
+    gB += stB;
   }
   cp_async_commit();
   gate();
 #pragma unroll
   for (int f = 0; f < CPD; ++f) {
     if (EDGE) fetchA(f);
-    else if (f <= fA_last) cp16s(cellA + f * 512, gA + f * stA, szA);
+    else if (f <= fA_last) cp16s(cellA + f * 512, gA, szA);
+    gA += stA;
     cp_async_commit();
   }
-  gA += CPD * stA;
-  gB += CPD * stB;
   // CPD + 1 groups issued; waiting for all but the newest CPD - 2 completes
   // ring B's group and A rows 0, 1
   cp_async_wait<CPD - 2>();

@@ -16,8 +16,10 @@ and runs continuous batching:
     its bytes return to the budget;
   - every pool is driven by its own host thread on its own CUDA streams, so the
     classes step independently and their work overlaps on the GPU; a thread
-    waits for each chunk of steps it queued before it admits, polls and queues
-    the next, so a new request waits at most one chunk.
+    keeps one chunk of steps queued ahead: it queues chunk i + 1, waits for
+    chunk i (a fence on the pool's stream), then polls, releases and admits,
+    so the pool's stream never drains while its host thread works, and a new
+    request waits at most two chunks.
 
 Latency of a request = completion time - arrival time (wall clock).
 """
@@ -181,6 +183,7 @@ class _RunState:
         self.lock = threading.Lock()
         self.cond = threading.Condition(self.lock)
         self.error = None
+        self.fences = {name: None for name in srv.classes}  # the queued chunk's fence per pool
         self.t0 = clock()
 
     def now(self):
@@ -242,14 +245,18 @@ class _RunState:
                     self.cond.notify_all()
 
     def service(self, name, sync):
-        """One round of class `name`: admit, step a chunk, poll and release."""
+        """One round of class `name`: admit, queue a chunk of steps, then (sync:
+        wait for the chunk queued in the previous round) poll and release."""
         self.admit(name)
         if not self.running[name]:
             return False
         pool = self.srv.pools[name]
         pool.step(self.srv.chunk)
         if sync:
-            pool.sync()
+            t = pool.fence()
+            if self.fences[name] is not None:
+                pool.fence_wait(self.fences[name])
+            self.fences[name] = t
         self.collect(name)
         return True
 

@@ -401,6 +401,17 @@ class Pool:
         check(lib().nls_pool_time_pass(self._p, j, iters, ctypes.byref(ms), ctypes.byref(pts)))
         return ms.value, pts.value
 
+    def fence(self) -> int:
+        """Ticket of the device work queued so far (steps and admissions)."""
+        t = ctypes.c_int32()
+        check(lib().nls_pool_fence(self._p, ctypes.byref(t)))
+        return t.value
+
+    def fence_wait(self, ticket: int):
+        """Block until the work before fence `ticket` has run; raises on a
+        slot's device-side failure as sync() does."""
+        check(lib().nls_pool_fence_wait(self._p, ticket))
+
     def time_passes(self, j0: int, j1: int, reps: int):
         """Mean duration (ms) of one Lanczos pass launch over passes j0..j1
         launched back to back as the step issues them, and the grid points

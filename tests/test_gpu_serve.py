@@ -49,3 +49,30 @@ def test_memory_budget_bounds_the_running_set():
             sol.run()
             traj, _ = sol.snapshots()
         assert np.array_equal(traj, r.traj), r.cls
+
+
+def test_pool_fences():
+    """nls_pool_fence / nls_pool_fence_wait: a fence waits for the steps queued
+    before it; only the last 16 fences can be waited on; a ticket never issued
+    is rejected."""
+    import nlsb200 as nl
+    from nlsb200 import workloads as W
+    sp, u0, v0, m, c = W.kg_case(64, 10.0, T=0.2, nt=20, ns=2, k=10, seed=3, precision=nl.FP32)
+    pool = nl.Pool(nl.KG_GAUTSCHI, 2, 10, nl.FP32, capacity_points=1 << 16, max_slots=1)
+    slot = pool.admit(sp, u0, v0, m)
+    pool.step(5)
+    t0 = pool.fence()
+    pool.fence_wait(t0)
+    assert pool.poll(slot)[0] >= 5
+    ts = [pool.fence() for _ in range(16)]
+    with pytest.raises(nl.NlsError):
+        pool.fence_wait(t0)  # recycled: older than the last 16
+    with pytest.raises(nl.NlsError):
+        pool.fence_wait(ts[-1] + 1)  # never issued
+    pool.fence_wait(ts[0])
+    pool.step(20)
+    pool.fence_wait(pool.fence())
+    pool.sync()
+    assert pool.poll(slot)[1]
+    pool.release(slot)
+    pool.close()

@@ -37,6 +37,13 @@ class FakePool:
         self.free.append(slot)
         return types.SimpleNamespace(traj=np.full(1, spec.tag))
 
+    def fence(self):
+        self.fences = getattr(self, "fences", 0) + 1
+        return self.fences
+
+    def fence_wait(self, ticket):
+        assert 0 < ticket <= self.fences
+
     def close(self):
         pass
 
