@@ -382,12 +382,14 @@ def run_reference(args, ws, rank, budget_s=150.0):
     return 0
 
 
-SERVE_RATES_HZ = (2.0, 8.0, 32.0)
+SERVE_RATES_HZ = (2.0, 8.0, 32.0, 128.0)
 SERVE_WINDOW_S = 4.0  # arrivals span about this long at each rate
 SERVE_REQUESTS = (12, 64)  # fewest and most requests of one rate's stream
 
 
 def _serve_once(serve, reqs, budget):
+    for r in reqs:
+        r.t_admit, r.t_done, r.slot, r.traj = float("nan"), float("nan"), -1, None
     srv = serve.Server(serve.default_classes(reqs, max_slots=32), chunk=20, memory_budget=budget)
     st = srv.run(reqs, timeout_s=600)
     srv.close()
@@ -401,25 +403,28 @@ def serving_leg(rates=SERVE_RATES_HZ, window_s=SERVE_WINDOW_S, steps=(500, 5000)
     64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D, 500-5000 steps each, Poisson
     arrivals) at each rate of `rates`: latency percentiles (arrival to last
     snapshot on the host) and aggregate throughput (all requests' grid-point
-    steps over the run's wall time). Each rate's stream holds rate x window_s
-    requests (at least 12, at most 64), so the highest rate keeps the server
-    loaded for most of its run. "saturated" serves the highest rate's requests
-    all arriving at once: the throughput ceiling of this mix on this server.
-    Admission by an 8 GiB device-memory budget shared by the class pools;
-    page-locked client snapshot buffers."""
+    steps over the run's wall time). One stream of 64 requests is drawn with
+    Poisson arrivals at 1 Hz; the stream of rate r is its first
+    rate x window_s requests (at least 12, at most 64) with the arrival times
+    divided by r, so the higher rates keep the server loaded for most of their
+    run. "saturated" serves all 64 requests arriving at once: the throughput
+    ceiling of this mix on this server. Admission by an 8 GiB device-memory
+    budget shared by the class pools; page-locked client snapshot buffers."""
     from nlsb200 import serve
     budget = int(budget_gib * (1 << 30))
     out = {"rates": [], "arrival_window_s": window_s, "steps_per_request": list(steps), "unit": UNIT,
            "memory_budget_bytes": budget, "snapshots_per_request": 5}
-    reqs = None
-    for i, rate in enumerate(rates):
+    reqs = serve.mixed_requests(SERVE_REQUESTS[1], 1.0, seed=seed, steps=steps, ns=5, pinned=True)
+    base = [r.arrival for r in reqs]
+    for rate in rates:
         count = int(min(max(round(rate * window_s), SERVE_REQUESTS[0]), SERVE_REQUESTS[1]))
-        reqs = serve.mixed_requests(count, rate, seed=seed + i, steps=steps, ns=5, pinned=True)
-        row = _serve_once(serve, reqs, budget)
+        for r, t in zip(reqs, base):
+            r.arrival = t / rate
+        row = _serve_once(serve, reqs[:count], budget)
         row["rate_hz"] = rate
         out["rates"].append(row)
-    for r in reqs:  # the last (highest) rate's requests, all at t = 0
-        r.arrival, r.t_admit, r.t_done, r.slot, r.traj = 0.0, float("nan"), float("nan"), -1, None
+    for r in reqs:
+        r.arrival = 0.0
     out["saturated"] = _serve_once(serve, reqs, budget)
     del reqs
     return out

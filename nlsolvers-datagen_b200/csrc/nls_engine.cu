@@ -111,11 +111,11 @@ bool pdl_on() {
   return v != 0;
 }
 template <typename K>
-cudaError_t pdl_launch(K kernel, dim3 grid, dim3 block, cudaStream_t st, const StepArgs &a) {
+cudaError_t pdl_launch(K kernel, dim3 grid, dim3 block, cudaStream_t st, const StepArgs &a, size_t smem = 0) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -169,18 +169,16 @@ cudaError_t launch2_sv(const StepArgs &a, int tiles, cudaStream_t st) {
 }
 
 // 3-D FP32 warp-marching passes (one block per strip, band, segment and
-// sequence of the block table).
+// sequence of the block table), launched with programmatic dependent launch
+// like the 2-D step kernels (each waits at entry).
 cudaError_t launch3_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k3_first_f32<<<tiles, 32 * BY3, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k3_first_f32, tiles, 32 * BY3, st, a);
 }
 cudaError_t launch3_final_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k3_final_f32<<<2 * tiles, 32 * FH3, 0, st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k3_final_f32, 2 * tiles, 32 * FH3, st, a);
 }
 cudaError_t launch3_lanczos_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  k3_lanczos_f32<<<tiles, 32 * W3, sizeof(Smem3), st>>>(a);
-  return cudaGetLastError();
+  return pdl_launch(k3_lanczos_f32, tiles, 32 * W3, st, a, sizeof(Smem3));
 }
 
 template <int DIM, typename E, int NSEQ, int SRC>

@@ -209,6 +209,7 @@ __device__ __forceinline__ void lz3f32_march(Smem3 &sm, int w, int lane, const f
 static __global__ void __launch_bounds__(32 * W3, 1) k3_lanczos_f32(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem3_raw[];
   Smem3 &sm = *reinterpret_cast<Smem3 *>(smem3_raw);
+  pdl_entry();
   if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
   const TileDesc t = a.tiles[blockIdx.x];
   const SlotDesc &s = a.slots[t.slot];
@@ -455,6 +456,7 @@ __device__ __forceinline__ void block_publish3(const StepArgs &a, const SlotDesc
 static __global__ void __launch_bounds__(32 * BY3) k3_first_f32(StepArgs a) {
   __shared__ double red[BY3][6];
   __shared__ int last_s;
+  pdl_entry();
   if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
   const TileDesc t = a.tiles[blockIdx.x];
   const SlotDesc &s = a.slots[t.slot];
@@ -505,6 +507,7 @@ static __global__ void __launch_bounds__(32 * FH3, 1) k3_final_f32(StepArgs a) {
   constexpr int NB = 8;
   __shared__ float Wsh[2][KMAX];
   __shared__ float Lsh[2];
+  pdl_entry();
   if ((int)(blockIdx.x >> 1) >= *a.ntiles) return;  // block-uniform
   const TileDesc t = a.tiles[blockIdx.x >> 1];
   const SlotDesc &s = a.slots[t.slot];
