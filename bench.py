@@ -387,46 +387,75 @@ SERVE_WINDOW_S = 4.0  # arrivals span about this long at each rate
 SERVE_REQUESTS = (12, 64)  # fewest and most requests of one rate's stream
 
 
-def _serve_once(serve, reqs, budget):
+def _serve_once(serve, reqs, budget, ws):
+    """Serve this rank's requests; the line's row aggregates every rank's
+    (grid-point-steps over the longest wall time, latencies of all requests)."""
     for r in reqs:
         r.t_admit, r.t_done, r.slot, r.traj = float("nan"), float("nan"), -1, None
-    srv = serve.Server(serve.default_classes(reqs, max_slots=32), chunk=20, memory_budget=budget)
-    st = srv.run(reqs, timeout_s=600)
-    srv.close()
-    row = st.summary()
-    row.update({"requests": len(reqs), "classes": sorted({r.cls for r in reqs}), "gp_steps": st.gp_steps})
+    barrier(ws)
+    if reqs:
+        srv = serve.Server(serve.default_classes(reqs, max_slots=32), chunk=20, memory_budget=budget)
+        st = srv.run(reqs, timeout_s=600)
+        srv.close()
+    else:
+        st = serve.ServeStats(completed=0, wall_s=0.0, gp_steps=0)
+    stats = [st]
+    if ws > 1:
+        import torch.distributed as dist
+        stats = [None] * ws
+        dist.all_gather_object(stats, st)
+    row = serve.merge_stats(stats) if ws > 1 else st.summary()
+    row.update({"requests": sum(s_.completed for s_ in stats),
+                "classes": sorted({r.cls for r in reqs}), "gp_steps": sum(s_.gp_steps for s_ in stats)})
     return row
 
 
-def serving_leg(rates=SERVE_RATES_HZ, window_s=SERVE_WINDOW_S, steps=(500, 5000), seed=5, budget_gib=8.0):
+def serving_leg(ws=1, rank=0, rates=SERVE_RATES_HZ, window_s=SERVE_WINDOW_S, steps=(500, 5000), seed=5,
+                budget_gib=8.0):
     """The serving mix (requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
     64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D, 500-5000 steps each, Poisson
-    arrivals) at each rate of `rates`: latency percentiles (arrival to last
-    snapshot on the host) and aggregate throughput (all requests' grid-point
-    steps over the run's wall time). One stream of 64 requests is drawn with
-    Poisson arrivals at 1 Hz; the stream of rate r is its first
-    rate x window_s requests (at least 12, at most 64) with the arrival times
-    divided by r, so the higher rates keep the server loaded for most of their
-    run. "saturated" serves all 64 requests arriving at once: the throughput
-    ceiling of this mix on this server. Admission by an 8 GiB device-memory
-    budget shared by the class pools; page-locked client snapshot buffers."""
+    arrivals) at each rate of `rates` per GPU: latency percentiles (arrival to
+    last snapshot on the host) and aggregate throughput (all requests'
+    grid-point-steps over the run's wall time). One stream of 64 requests per
+    GPU is drawn with Poisson arrivals at 1 Hz per GPU; the stream of rate r is
+    its first rate x window_s requests per GPU (at least 12, at most 64) with
+    the arrival times divided by r, so the higher rates keep the servers loaded
+    for most of their run. With several GPUs each rate's stream is placed on
+    them by grid-point-steps (serve.partition, largest first) and every rank
+    serves its share with its own server (weak scaling: the stream grows with
+    the GPUs). "saturated" serves the whole stream arriving at once: the
+    throughput ceiling of this mix on these servers. Admission by an 8 GiB
+    device-memory budget per GPU shared by its class pools; page-locked client
+    snapshot buffers."""
     from nlsb200 import serve
     budget = int(budget_gib * (1 << 30))
     out = {"rates": [], "arrival_window_s": window_s, "steps_per_request": list(steps), "unit": UNIT,
-           "memory_budget_bytes": budget, "snapshots_per_request": 5}
-    reqs = serve.mixed_requests(SERVE_REQUESTS[1], 1.0, seed=seed, steps=steps, ns=5, pinned=True)
-    base = [r.arrival for r in reqs]
+           "memory_budget_bytes": budget, "snapshots_per_request": 5, "n_gpus": ws,
+           "placement": "greedy by grid-point-steps" if ws > 1 else "one GPU"}
+    plans = serve.mixed_plans(SERVE_REQUESTS[1] * ws, float(ws), seed=seed, steps=steps)
+    base = {pl.rid: pl.arrival for pl in plans}
+    built = {}
+
+    def mine(sub):
+        part = serve.partition(sub, ws)[rank]
+        for pl in part:
+            if pl.rid not in built:
+                built[pl.rid] = serve.build_request(pl, ns=5, pinned=True)
+        return [built[pl.rid] for pl in part]
+
     for rate in rates:
-        count = int(min(max(round(rate * window_s), SERVE_REQUESTS[0]), SERVE_REQUESTS[1]))
-        for r, t in zip(reqs, base):
-            r.arrival = t / rate
-        row = _serve_once(serve, reqs[:count], budget)
+        count = int(min(max(round(rate * window_s), SERVE_REQUESTS[0]), SERVE_REQUESTS[1])) * ws
+        reqs = mine(plans[:count])
+        for r in reqs:
+            r.arrival = base[r.rid] / rate
+        row = _serve_once(serve, reqs, budget, ws)
         row["rate_hz"] = rate
         out["rates"].append(row)
+    reqs = mine(plans)
     for r in reqs:
         r.arrival = 0.0
-    out["saturated"] = _serve_once(serve, reqs, budget)
-    del reqs
+    out["saturated"] = _serve_once(serve, reqs, budget, ws)
+    built.clear()
     return out
 
 
@@ -675,8 +704,8 @@ def run_ours(args, ws, rank, lrank):
         "kernels_per_step": kernels,
         "clocks": clk.summary(),
     }
-    if ws == 1 and not args.no_serve:
-        line["serving"] = serving_leg()
+    if not args.no_serve:
+        line["serving"] = serving_leg(ws, rank)
     if ws == 1 and not args.no_other:
         line["other_configs"] = other_configs_leg()
     if ws == 1 and rank == 0 and not args.no_cpu:

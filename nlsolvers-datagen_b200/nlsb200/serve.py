@@ -315,15 +315,34 @@ class _RunState:
             raise self.error
 
 
-def mixed_requests(count: int, rate_hz: float, seed: int = 0, steps=(500, 5000), scale: float = 1.0,
-                   ns: int = 10, pinned: bool = False) -> list[Request]:
-    """The serving mix: requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
-    64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D (u_tt = Lu + u - u^3 + sigma xi,
-    sigma ~ U(0.05, 0.5), discrete noise sigma xi / sqrt(dt dx^d) with Philox
-    keyed by (seed, step, point)); Poisson arrivals at rate_hz; step counts
-    uniform in `steps`. `scale` shrinks the grid edges (for short runs).
-    pinned: each request brings page-locked snapshot buffers (a client that
-    allocated them ahead), so admission registers no memory."""
+@dataclass
+class RequestPlan:
+    """The drawn parameters of one request of the serving mix (no fields yet)."""
+    rid: int
+    cls: str
+    arrival: float
+    n: int
+    nt: int
+    seed: int
+    sigma: float = 0.0
+
+    @property
+    def dim(self) -> int:
+        return 3 if self.cls == "kg3d" else 2
+
+    @property
+    def gp_steps(self) -> int:
+        return self.n ** self.dim * (self.nt - 1)
+
+    def padded_points(self) -> int:
+        n = ((self.n + 31) // 32 * 32) * self.n * (self.n if self.dim == 3 else 1)
+        return (n + 255) // 256 * 256
+
+
+def mixed_plans(count: int, rate_hz: float, seed: int = 0, steps=(500, 5000), scale: float = 1.0) -> list[RequestPlan]:
+    """The random draws of the serving mix, in the order mixed_requests makes
+    them: per request the arrival gap, the class, the step count, the field
+    seed, the grid edge (and sigma for phi^4)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -333,32 +352,120 @@ def mixed_requests(count: int, rate_hz: float, seed: int = 0, steps=(500, 5000),
         nt = int(rng.integers(steps[0], steps[1] + 1)) + 1
         s = int(rng.integers(1 << 30))
         if kind == "kg2d":
-            n = max(16, int(rng.integers(64, 301) * scale))
-            spec, u0, v0, m, c = W.kg_case(n, 10.0, T=0.01 * nt, nt=nt, ns=ns, k=10, seed=s, precision=FP32)
+            n, sigma = max(16, int(rng.integers(64, 301) * scale)), 0.0
         elif kind == "nlse2d":
-            n = max(16, int(rng.integers(64, 257) * scale))
-            spec, u0, v0, m, c = W.nlse_case(n, 10.0, T=1e-3 * nt, nt=nt, ns=ns, k=12, seed=s, precision=FP32)
+            n, sigma = max(16, int(rng.integers(64, 257) * scale)), 0.0
         elif kind == "kg3d":
-            n = max(12, int(rng.integers(64, 161) * scale))
-            spec, u0, v0, m, c = W.kg_case(n, 10.0, T=0.01 * nt, nt=nt, ns=ns, k=10, seed=s, dim=3,
-                                           precision=FP32)
+            n, sigma = max(12, int(rng.integers(64, 161) * scale)), 0.0
         else:
             n = max(16, int(rng.integers(64, 301) * scale))
-            spec, u0, v0, m, c = W.kg_case(n, 10.0, T=0.01 * nt, nt=nt, ns=ns, k=10, seed=s, method=SP4_SV,
-                                           precision=FP32, kinks=True)
-            sigma = rng.uniform(0.05, 0.5)
-            dx = 2 * 10.0 / (n - 1)
-            spec.p1, spec.q1, spec.p3, spec.q3 = 0.0, 1.0, 0.0, -1.0
-            spec.rm, spec.r0 = 0.0, sigma / math.sqrt(spec.dt * dx ** 2)
-            m = np.ones(u0.shape)
-        c = None
-        req = Request(i, kind, t, spec, u0, v0, m, c)
-        if pinned:
-            dt = np.complex128 if spec.complex else np.float64
-            req.out_traj = pinned_empty((spec.ns,) + spec.shape, dt)
-            if not spec.complex:
-                req.out_vel = pinned_empty((spec.ns,) + spec.shape)
-        out.append(req)
+            sigma = float(rng.uniform(0.05, 0.5))
+        out.append(RequestPlan(i, kind, t, n, nt, s, sigma))
+    return out
+
+
+def build_request(pl: RequestPlan, ns: int = 10, pinned: bool = False) -> Request:
+    """The request of a plan: its problem and seeded fields (and, pinned, its
+    page-locked snapshot buffers)."""
+    nt, s, n = pl.nt, pl.seed, pl.n
+    if pl.cls == "kg2d":
+        spec, u0, v0, m, c = W.kg_case(n, 10.0, T=0.01 * nt, nt=nt, ns=ns, k=10, seed=s, precision=FP32)
+    elif pl.cls == "nlse2d":
+        spec, u0, v0, m, c = W.nlse_case(n, 10.0, T=1e-3 * nt, nt=nt, ns=ns, k=12, seed=s, precision=FP32)
+    elif pl.cls == "kg3d":
+        spec, u0, v0, m, c = W.kg_case(n, 10.0, T=0.01 * nt, nt=nt, ns=ns, k=10, seed=s, dim=3, precision=FP32)
+    else:
+        spec, u0, v0, m, c = W.kg_case(n, 10.0, T=0.01 * nt, nt=nt, ns=ns, k=10, seed=s, method=SP4_SV,
+                                       precision=FP32, kinks=True)
+        dx = 2 * 10.0 / (n - 1)
+        spec.p1, spec.q1, spec.p3, spec.q3 = 0.0, 1.0, 0.0, -1.0
+        spec.rm, spec.r0 = 0.0, pl.sigma / math.sqrt(spec.dt * dx ** 2)
+        m = np.ones(u0.shape)
+    req = Request(pl.rid, pl.cls, pl.arrival, spec, u0, v0, m, None)
+    if pinned:
+        dt = np.complex128 if spec.complex else np.float64
+        req.out_traj = pinned_empty((spec.ns,) + spec.shape, dt)
+        if not spec.complex:
+            req.out_vel = pinned_empty((spec.ns,) + spec.shape)
+    return req
+
+
+def mixed_requests(count: int, rate_hz: float, seed: int = 0, steps=(500, 5000), scale: float = 1.0,
+                   ns: int = 10, pinned: bool = False) -> list[Request]:
+    """The serving mix: requests uniform over KG 2-D 64^2-300^2, NLSE 2-D
+    64^2-256^2, KG 3-D 64^3-160^3 and phi^4 2-D (u_tt = Lu + u - u^3 + sigma xi,
+    sigma ~ U(0.05, 0.5), discrete noise sigma xi / sqrt(dt dx^d) with Philox
+    keyed by (seed, step, point)); Poisson arrivals at rate_hz; step counts
+    uniform in `steps`. `scale` shrinks the grid edges (for short runs).
+    pinned: each request brings page-locked snapshot buffers (a client that
+    allocated them ahead), so admission registers no memory."""
+    return [build_request(pl, ns, pinned) for pl in mixed_plans(count, rate_hz, seed, steps, scale)]
+
+
+# ------------------------------------------------------------ several GPUs
+# Trajectories never interact, so requests are partitioned across GPUs and
+# every GPU runs its own server (one process per GPU, its own pools, streams
+# and graphs); nothing crosses NVLink on the hot path.
+
+def plan_bytes(pl: RequestPlan) -> int:
+    """Device bytes of a plan's request (padded points x its class's bytes per point)."""
+    meth = {"kg2d": KG_GAUTSCHI, "nlse2d": NLSE_SS2, "kg3d": KG_GAUTSCHI, "phi4_2d": SP4_SV}[pl.cls]
+    k = {"kg2d": 10, "nlse2d": 12, "kg3d": 10, "phi4_2d": 3}[pl.cls]
+    return pl.padded_points() * bytes_per_point(meth, k, FP32)
+
+
+def partition(plans, ndev: int, key: str = "work") -> list[list]:
+    """Greedy placement of requests on ndev GPUs, largest first: each goes to
+    the GPU with the least load so far. key "work": load = grid-point-steps
+    (balances the GPUs' busy time); "bytes": load = device bytes, the
+    bin-packing of n (k-1) s of the memory budget. Within a GPU the requests
+    keep their arrival order. Deterministic: every rank computes the same
+    placement from the same plans."""
+    if ndev < 1:
+        raise ValueError("ndev must be at least 1")
+    weight = (lambda p: p.gp_steps) if key == "work" else plan_bytes if key == "bytes" else None
+    if weight is None:
+        raise ValueError(f"unknown placement key {key!r}")
+    load = [0] * ndev
+    parts = [[] for _ in range(ndev)]
+    for pl in sorted(plans, key=lambda p: (-weight(p), p.rid)):
+        d = min(range(ndev), key=lambda i: (load[i], i))
+        load[d] += weight(pl)
+        parts[d].append(pl)
+    for part in parts:
+        part.sort(key=lambda p: (p.arrival, p.rid))
+    return parts
+
+
+def serve_rank(plans, rank: int, world: int, key: str = "work", ns: int = 10, pinned: bool = False,
+               classes=None, **server_kw) -> tuple[list[Request], ServeStats]:
+    """The share of GPU `rank` of a stream placed over `world` GPUs: builds only
+    its own requests and serves them with a Server on the current device (the
+    caller selects it, one process per GPU). Returns the requests (with their
+    results) and the rank's stats; the aggregate over ranks is the sum of
+    grid-point-steps over the longest wall time."""
+    mine = partition(plans, world, key)[rank]
+    reqs = [build_request(pl, ns, pinned) for pl in mine]
+    if not reqs:
+        return [], ServeStats(completed=0, wall_s=0.0, gp_steps=0)
+    srv = Server(classes or default_classes(reqs), **server_kw)
+    try:
+        st = srv.run(reqs)
+    finally:
+        srv.close()
+    return reqs, st
+
+
+def merge_stats(stats: list[ServeStats]) -> dict:
+    """Aggregate of per-GPU stats: completed requests, grid-point-steps over the
+    longest wall time, latency percentiles over all requests."""
+    lat = [x for st in stats for x in st.latencies_s]
+    merged = ServeStats(completed=sum(st.completed for st in stats), wall_s=max(st.wall_s for st in stats),
+                        gp_steps=sum(st.gp_steps for st in stats), latencies_s=lat,
+                        peak_bytes=max(st.peak_bytes for st in stats))
+    out = merged.summary()
+    out["per_gpu_gp_steps"] = [st.gp_steps for st in stats]
+    out["per_gpu_wall_s"] = [st.wall_s for st in stats]
     return out
 
 

@@ -76,3 +76,21 @@ def test_pool_fences():
     assert pool.poll(slot)[1]
     pool.release(slot)
     pool.close()
+
+
+def test_rank_share_of_a_placed_stream():
+    """serve_rank on one GPU: the share of rank 0 of a stream placed over two
+    GPUs completes, and its results equal solo runs bitwise (each GPU of a
+    multi-GPU server runs the same Server over its own requests)."""
+    import nlsb200 as nl
+    from nlsb200 import serve
+    plans = serve.mixed_plans(12, 200.0, seed=21, steps=(30, 80), scale=0.3)
+    share = serve.partition(plans, 2)[0]
+    reqs, st = serve.serve_rank(plans, 0, 2, ns=3, chunk=8, memory_budget=1 << 30)
+    assert [r.rid for r in reqs] == [p.rid for p in share]
+    assert st.completed == len(share) and st.gp_steps == sum(p.gp_steps for p in share)
+    for r in reqs[:3]:
+        with nl.Solver(r.spec, r.u0, r.v0, r.m, r.c) as sol:
+            sol.run()
+            traj, _ = sol.snapshots()
+        assert np.array_equal(traj, r.traj), r.cls
