@@ -318,9 +318,11 @@ int nls_set_device(int32_t device);
    and issues no host-to-device copy. It launches its kernels on `stream` (a
    cudaStream_t; NULL: the legacy stream), then copies one device status word
    to the host and synchronises `stream`, and returns after the steps
-   completed. The first call on a device does the set-up (loads the kernels
-   and looks up the scratch address); make that first call before any stream
-   capture. Every call re-initialises what must start at zero (reduction
+   completed. It cannot be captured into a CUDA graph: a call on a stream that
+   is being captured (or while a global-mode capture runs) returns
+   NLS_ERR_STATE before it enqueues anything, so the capture stays valid. The
+   first call on a device does the set-up (loads the kernels and looks up the
+   scratch address). Every call re-initialises what must start at zero (reduction
    tickets, step state), so nothing needs clearing between calls. All calls on
    one device share the scratch: calls that overlap in time (from several
    threads or streams) race and must be serialised by the caller. On

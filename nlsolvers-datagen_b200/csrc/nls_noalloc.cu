@@ -354,6 +354,17 @@ extern "C" int nls_gautschi_step_noalloc(const nls_problem *p, double *u, double
   }
   if (nsteps == 0) return NLS_OK;
   cudaStream_t st = (cudaStream_t)stream;
+  // The call ends with a device-to-host copy of the status word and a stream
+  // synchronisation, neither of which a CUDA graph capture allows: refuse a
+  // capturing stream before anything is enqueued, so the caller's capture
+  // stays valid.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  const cudaError_t ce = cudaStreamIsCapturing(st, &cap);
+  if (ce != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return fail(NLS_ERR_STATE, "nls_gautschi_step_noalloc cannot be captured into a CUDA graph (it copies its "
+                               "status to the host and synchronises its stream); call it outside a capture");
+  }
   if (p->precision == NLS_FP64) return run<double>(*p, u, u_past, m, c, first_step, nsteps, st);
   return run<float>(*p, u, u_past, m, c, first_step, nsteps, st);
 }

@@ -181,3 +181,39 @@ def test_noalloc_rejects_step_counter_overflow():
     nl.lib().nls_last_error(msg, 512)
     assert b"step counter" in msg.value
     assert nl.lib().nls_gautschi_step_noalloc(ctypes.byref(_p(sp)), ptr, ptr, ptr, None, 0, -1, None) == -1
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_capturing_stream(device_in_use):
+    """Inside a CUDA graph capture the call returns NLS_ERR_STATE before it
+    enqueues anything (it would copy its status to the host and synchronise),
+    so the caller's capture stays valid and replays; outside it runs."""
+    import torch
+    nl = _nl()
+    spec, u0, v0, m, _ = _case(nl.KG_GAUTSCHI, "fp64", False, n=64)
+    dev = torch.device("cuda:0")
+    md = torch.tensor(m, dtype=torch.float64, device=dev)
+    ua = torch.tensor(u0, dtype=torch.float64, device=dev)
+    upa = torch.tensor(u0 - spec.dt * v0, dtype=torch.float64, device=dev)
+    x = torch.zeros(4, device=dev)
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        x.add_(1)  # warm-up outside the capture
+    torch.cuda.current_stream().wait_stream(side)
+    err = None
+    with torch.cuda.graph(g):
+        x.add_(1)
+        try:
+            _noalloc(spec, ua, upa, md, None, 1, 1)
+        except nl.NlsError as ex:
+            err = ex
+    assert err is not None and err.code == -7, err
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.all(x == 2)
+    u_before = ua.clone()
+    _noalloc(spec, ua, upa, md, None, 1, 1)
+    torch.cuda.synchronize()
+    assert not torch.equal(u_before, ua) and torch.all(torch.isfinite(ua))
