@@ -172,7 +172,7 @@ cudaError_t launch2_sv(const StepArgs &a, int tiles, cudaStream_t st) {
 // sequence of the block table), launched with programmatic dependent launch
 // like the 2-D step kernels (each waits at entry).
 cudaError_t launch3_first_f32(const StepArgs &a, int tiles, cudaStream_t st) {
-  return pdl_launch(k3_first_f32, tiles, 32 * BY3, st, a);
+  return pdl_launch(k3_first_f32, tiles, 32 * BY3, st, a, SMEM_FIRST3);
 }
 cudaError_t launch3_final_f32(const StepArgs &a, int tiles, cudaStream_t st) {
   return pdl_launch(k3_final_f32, 2 * tiles, 32 * FH3, st, a);
@@ -230,6 +230,7 @@ template <int DIM, typename R> cudaError_t attrs_real() {
   cudaError_t e;
   if constexpr (DIM == 3 && sizeof(R) == 4) {
     if ((e = set_smem(k3_lanczos_f32, sizeof(Smem3)))) return e;
+    if ((e = set_smem(k3_first_f32, SMEM_FIRST3))) return e;
   }
   if ((e = set_smem(k_first<DIM, R, 2, SRC_KG>, smem_first<DIM, R, 2>()))) return e;
   if ((e = set_smem(k_lanczos<DIM, R, 2>, smem_lanczos<DIM, R, 2>()))) return e;

@@ -344,45 +344,65 @@ __device__ __forceinline__ F4 src3(const F4 &u, const F4 &m, const SlotDesc &s, 
   return x;
 }
 
+// The first pass's rows (u, and m for the sinc sequence, of the warp's own row
+// and the rows above and below) stream through a per-warp cp.async ring of
+// RF3 planes in shared memory: each lane copies its own 16 bytes and later reads
+// back only what it copied, so no barrier is needed, and RF3 - 2 planes are in
+// flight while a plane's stencil is formed (with loads only one plane ahead in
+// registers, the march waited for a memory round trip at every plane).
+constexpr int RF3 = 4;                                // planes per ring
+constexpr int NRF3 = 6;                               // rows per plane: u (own, above, below), then m
+constexpr uint32_t FRP3 = NRF3 * 512;                 // bytes of one plane of a warp's ring
+constexpr size_t SMEM_FIRST3 = (size_t)BY3 * RF3 * FRP3;
+
 template <int SQ>
 __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &s, const Strip3 &S, int y, int p0,
-                                             int p1, int step, const F4 &OPx, const F4 &miss0, double *acc) {
+                                             int p1, int step, const F4 &OPx, const F4 &miss0, double *acc,
+                                             uint32_t cell) {
   const int nx = s.nx, ny = s.ny, nz = s.nz;
   const long long P = s.pitch, PS = P * ny;
   const long long row_off = s.off + (long long)y * P + S.col0;
   const float *pU = (const float *)a.f.u_hi + row_off;
   const float *pM = (const float *)a.f.m + row_off;
+  const float *safe = (const float *)a.f.u_hi + s.off;  // source of zero-filled copies
   float *pV = (float *)a.V + (long long)(SQ * a.kv) * a.vstride + row_off;
   const bool hu = y > 0, hd = y < ny - 1;
   const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
-  // raw rows (u, and m for the sinc sequence) are loaded one plane ahead of
-  // the plane whose stencil needs them, so a plane's loads overlap the
-  // previous plane's arithmetic
-  struct Raw {
-    F4 u, m;
-    int q;
-    long long dy;
+  // fetch f: plane p0-1+f, rows dy = 0, -1, +1 (and their m) into ring slot
+  // f % RF3; rows outside the grid are zero-filled by the copy itself
+  auto fetch = [&](int f) {
+    const int q = p0 - 1 + f;
+    const uint32_t base = cell + (uint32_t)((f % RF3) * FRP3);
+    const bool qok = S.ld && q >= 0 && q < nz;
+    const long long o = (long long)q * PS;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int dy = r == 0 ? 0 : (r == 1 ? -1 : 1);
+      const bool ok = qok && (dy == 0 || (dy < 0 ? hu : hd));
+      cp16z(base + r * 512, ok ? (const void *)(pU + o + dy * P) : (const void *)safe, ok);
+      if (SQ == 1) cp16z(base + (3 + r) * 512, ok ? (const void *)(pM + o + dy * P) : (const void *)safe, ok);
+    }
+    cp_async_commit();
   };
-  auto load = [&](int q, long long dy) -> Raw {
+  // source row of plane q, row dy, from ring slot f % RF3
+  auto make = [&](int f, int q, int r) -> F4 {
+    const int dy = r == 0 ? 0 : (r == 1 ? -1 : 1);
+    const uint32_t base = cell + (uint32_t)((f % RF3) * FRP3);
+    const F4 u = lds16(base + r * 512);
+    const F4 m = SQ == 1 ? lds16(base + (3 + r) * 512) : F4{f2(0.f), f2(0.f)};
     const bool ok = S.ld && q >= 0 && q < nz && (dy == 0 || (dy < 0 ? hu : hd));
-    const long long o = (long long)q * PS + dy * P;
-    Raw r{ldrow(pU + o, ok), SQ == 1 ? ldrow(pM + o, ok) : F4{f2(0.f), f2(0.f)}, q, dy};
-    return r;
+    return src3<SQ>(u, m, s, step, S.col0, nx, ((long long)q * ny + y + dy) * nx, noisy, ok);
   };
-  auto make = [&](const Raw &r) -> F4 {
-    const bool ok = S.ld && r.q >= 0 && r.q < nz && (r.dy == 0 || (r.dy < 0 ? hu : hd));
-    return src3<SQ>(r.u, r.m, s, step, S.col0, nx, ((long long)r.q * ny + y + r.dy) * nx, noisy, ok);
-  };
-  F4 Xm = make(load(p0 - 1, 0)), Xo = make(load(p0, 0));
-  Raw Rp = load(p0 + 1, 0), Ru = load(p0, -1), Rd = load(p0, 1);
+#pragma unroll
+  for (int f = 0; f < RF3; ++f) fetch(f);
+  cp_async_wait<RF3 - 2>();  // fetches 0, 1 (planes p0-1, p0) landed
+  F4 Xm = make(0, p0 - 1, 0), Xo = make(1, p0, 0);
   float2 q1 = f2(0.f), q3 = f2(0.f), q4 = f2(0.f);
   for (int q = p0; q < p1; ++q) {
-    const F4 Xp = make(Rp), Xu = make(Ru), Xd = make(Rd);
-    if (q + 1 < p1) {
-      Rp = load(q + 2, 0);
-      Ru = load(q + 1, -1);
-      Rd = load(q + 1, 1);
-    }
+    const int i = q - p0;
+    cp_async_wait<RF3 - 3>();  // fetch i + 2 (plane q + 1) landed
+    const F4 Xp = make(i + 2, q + 1, 0), Xu = make(i + 1, q, 1), Xd = make(i + 1, q, 2);
+    fetch(i + RF3);  // plane q + RF3 - 1 into the slot of plane q - 1, read in earlier iterations
     const float lft = __shfl_up_sync(0xffffffffu, Xo.b.y, 1);
     const float rgt = __shfl_down_sync(0xffffffffu, Xo.a.x, 1);
     const float2 zm = f2(float((q == 0) + (q == nz - 1)));
@@ -401,6 +421,7 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
     Xm = Xo;
     Xo = Xp;
   }
+  cp_async_wait<0>();
   acc[1] += (double)(q1.x + q1.y);
   acc[3] += (double)(q3.x + q3.y);
   acc[4] += (double)(q4.x + q4.y);
@@ -453,9 +474,10 @@ __device__ __forceinline__ void block_publish3(const StepArgs &a, const SlotDesc
   }
 }
 
-static __global__ void __launch_bounds__(32 * BY3) k3_first_f32(StepArgs a) {
+static __global__ void __launch_bounds__(32 * BY3, 1) k3_first_f32(StepArgs a) {
   __shared__ double red[BY3][6];
   __shared__ int last_s;
+  extern __shared__ __align__(16) unsigned char ring3f[];  // SMEM_FIRST3 bytes: one ring per warp
   pdl_entry();
   if ((int)blockIdx.x >= *a.ntiles) return;  // block-uniform
   const TileDesc t = a.tiles[blockIdx.x];
@@ -479,9 +501,10 @@ static __global__ void __launch_bounds__(32 * BY3) k3_first_f32(StepArgs a) {
     miss0 = F4{make_float2(m[0], m[1]), make_float2(m[2], m[3])};
   }
   double acc[6] = {0, 0, 0, 0, 0, 0};
+  const uint32_t cell = (uint32_t)__cvta_generic_to_shared(ring3f + (size_t)w * RF3 * FRP3 + lane * 16);
   if (y < ny) {  // warp-uniform
-    if (sq == 0) first3_march<0>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc);
-    else first3_march<1>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc);
+    if (sq == 0) first3_march<0>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc, cell);
+    else first3_march<1>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc, cell);
   }
   const bool keep = y < ny && S.io;
 #pragma unroll
