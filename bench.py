@@ -53,6 +53,7 @@ FALLBACK_HBM = 6650.0
 # profiles/ncu_lanczos_pass_kg2d.md; algorithmic: 24 B per point.
 TRAFFIC_BYTES_PER_POINT_PASS = 17.79
 TIMED_REGION_S = 1.0
+FINAL_ROWS = 25  # rows per tile of the 2-D final pass
 
 
 def workload_config(k, ws, B):
@@ -608,10 +609,12 @@ def run_ours(args, ws, rank, lrank):
     n = cases[0][0].n
     cap = sum(((s.nx + 31) // 32 * 32) * s.ny for s, *_ in cases) + 256 * B
 
-    # the final pass sums nothing across tiles and keeps its own 16-row tiles
+    # the final pass sums nothing across tiles and keeps its own 25-row tiles
+    # (one wave of warps for the batch; 12 / 16 / 20 / 25 / 30 rows measured
+    # 0.346 / 0.345 / 0.358 / 0.340 / 0.346 ms per step with 28-row passes)
     # (more warps than the passes' segments give it)
     def make_pool(seg):
-        return Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=seg, final_segment=16)
+        return Pool(KG_GAUTSCHI, 2, k, FP32, capacity_points=cap, max_slots=B, segment=seg, final_segment=FINAL_ROWS)
 
     def admit_all(pool):
         for cs in cases:
@@ -621,7 +624,7 @@ def run_ours(args, ws, rank, lrank):
     # = 2304 warps, one wave of 16 warps on each of the 148 SMs
     seg, seg_times = autotune.choose_segment(make_pool, admit_all, candidates=(16, 25, 28, 32), steps=6)
     seg = bcast_int(seg, ws)  # every rank runs rank 0's tiling
-    tuning.update({"segment_rows": seg, "final_segment_rows": 16, "segment_ms": seg_times})
+    tuning.update({"segment_rows": seg, "final_segment_rows": FINAL_ROWS, "segment_ms": seg_times})
     pool = make_pool(seg)
     admit_all(pool)
     pool.step(args.warmup)
