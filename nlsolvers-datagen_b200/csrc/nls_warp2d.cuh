@@ -1717,6 +1717,8 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
                                                 bool store, Gate &&gate) {
   const F4 zero4 = F4{f2(0.f), f2(0.f)};
   const float2 P1 = f2(float(s.p1)), Q1 = f2(float(s.q1)), P3 = f2(float(s.p3)), Q3 = f2(float(s.q3));
+  // SQ 2: the sinc sequence with the polynomial force and no noise (the loop
+  // holds only that arithmetic, which keeps its code small)
   const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
   auto rowU = [&](int r) -> F4 {
     const bool ok = EDGE ? (ld && r >= 0 && r < ny && r <= r1) : (ld && r <= r1);
@@ -1730,6 +1732,7 @@ __device__ __forceinline__ void first_f32_march(const float *pU, const float *pM
   // source row r from its raw rows (g and noise for sequence 1; zero outside the grid)
   auto make = [&](const F4 &u, const F4 &m, int r) -> F4 {
     if (SQ == 0) return u;
+    if (SQ == 2) return f4_g(u, m, P1, Q1, P3, Q3);
     F4 x = f4_force(s.nl_kind, u, m, s, P1, Q1, P3, Q3);
     if (noisy && r >= 0 && r < ny) {
       float xs[4] = {x.a.x, x.a.y, x.b.x, x.b.y};
@@ -1836,6 +1839,10 @@ __device__ __forceinline__ void first_f32_body(const StepArgs &a, const TileDesc
     const bool st = !a.v0_u;
     if (inner) first_f32_march<false, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st, gate);
     else first_f32_march<true, 0>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, st, gate);
+  } else if (s.nl_kind == NL_POLY && s.rm == 0.0 && s.r0 == 0.0) {
+    // polynomial force, no noise (KG)
+    if (inner) first_f32_march<false, 2>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, true, gate);
+    else first_f32_march<true, 2>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, true, gate);
   } else {
     if (inner) first_f32_march<false, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, true, gate);
     else first_f32_march<true, 1>(pU, pM, pV, P, r0, r1, ny, ld, io, s, S, step, OPx, xmiss, acc, true, gate);
