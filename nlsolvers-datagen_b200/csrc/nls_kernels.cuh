@@ -890,21 +890,25 @@ __device__ bool ftri_fast(int k, const double *d, const double *e, int lane, int
   double u = 0.0;
   {
     double p0 = 1.0, p1 = d[0] - lam1, E = 1.0, sg = 1.0;
+    double num = 1.0, den = 1.0;  // u_lane = num / den, one division per lane after the recurrence
     bool ok = true;
-    if (lane == 0) u = 1.0;
 #pragma unroll
     for (int i = 1; i < KP; ++i) {
       if (i < k) {
         E *= e[i - 1];
         sg = -sg;
         ok = ok && e[i - 1] > 1e-150;
-        if (i == lane) u = sg * p1 / E;
+        if (i == lane) {
+          num = sg * p1;
+          den = E;
+        }
         const double p2 = (d[i] - lam1) * p1 - e[i - 1] * e[i - 1] * p0;
         p0 = p1;
         p1 = p2;
       }
     }
     if (!ok) return false;
+    if (lane < k) u = lane == 0 ? 1.0 : num / den;
   }
   double uu = u * u;
 #pragma unroll
@@ -997,7 +1001,8 @@ __device__ __forceinline__ void ftri_reg_body(const StepArgs &a, int gw, int *do
   const double ftr = a.tsc[sq][0] * s.dt, fti = a.tsc[sq][1] * s.dt;
   double cr = 0.0, ci = 0.0;
   int status = 0;
-  if (!ftri_fast<KP>(k, d, e, lane, fk, ftr, fti, cr, ci)) {
+  // the QL sweeps below are the rare fallback: laid out off the hot path
+  if (__builtin_expect(!ftri_fast<KP>(k, d, e, lane, fk, ftr, fti, cr, ci), 0)) {
   double Z[KP];
 #pragma unroll
   for (int i = 0; i < KP; ++i) Z[i] = i == lane ? 1.0 : 0.0;

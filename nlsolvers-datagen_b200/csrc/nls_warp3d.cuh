@@ -328,6 +328,7 @@ template <int SQ>
 __device__ __forceinline__ F4 src3(const F4 &u, const F4 &m, const SlotDesc &s, int step, int col0, int nx,
                                    long long row_pt, bool noisy, bool ok) {
   if (SQ == 0) return u;
+  if (SQ == 2) return f4_g(u, m, f2(float(s.p1)), f2(float(s.q1)), f2(float(s.p3)), f2(float(s.q3)));
   F4 x = f4_force(s.nl_kind, u, m, s, f2(float(s.p1)), f2(float(s.q1)), f2(float(s.p3)), f2(float(s.q3)));
   if (noisy && ok) {
     float xs[4] = {x.a.x, x.a.y, x.b.x, x.b.y};
@@ -365,7 +366,7 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
   const float *pU = (const float *)a.f.u_hi + row_off;
   const float *pM = (const float *)a.f.m + row_off;
   const float *safe = (const float *)a.f.u_hi + s.off;  // source of zero-filled copies
-  float *pV = (float *)a.V + (long long)(SQ * a.kv) * a.vstride + row_off;
+  float *pV = (float *)a.V + (long long)((SQ >= 1 ? 1 : 0) * a.kv) * a.vstride + row_off;
   const bool hu = y > 0, hd = y < ny - 1;
   const bool noisy = SQ == 1 && (s.rm != 0.0 || s.r0 != 0.0);
   // fetch f: plane p0-1+f, rows dy = 0, -1, +1 (and their m) into ring slot
@@ -380,7 +381,7 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
       const int dy = r == 0 ? 0 : (r == 1 ? -1 : 1);
       const bool ok = qok && (dy == 0 || (dy < 0 ? hu : hd));
       cp16z(base + r * 512, ok ? (const void *)(pU + o + dy * P) : (const void *)safe, ok);
-      if (SQ == 1) cp16z(base + (3 + r) * 512, ok ? (const void *)(pM + o + dy * P) : (const void *)safe, ok);
+      if (SQ >= 1) cp16z(base + (3 + r) * 512, ok ? (const void *)(pM + o + dy * P) : (const void *)safe, ok);
     }
     cp_async_commit();
   };
@@ -389,7 +390,7 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
     const int dy = r == 0 ? 0 : (r == 1 ? -1 : 1);
     const uint32_t base = cell + (uint32_t)((f % RF3) * FRP3);
     const F4 u = lds16(base + r * 512);
-    const F4 m = SQ == 1 ? lds16(base + (3 + r) * 512) : F4{f2(0.f), f2(0.f)};
+    const F4 m = SQ >= 1 ? lds16(base + (3 + r) * 512) : F4{f2(0.f), f2(0.f)};
     const bool ok = S.ld && q >= 0 && q < nz && (dy == 0 || (dy < 0 ? hu : hd));
     return src3<SQ>(u, m, s, step, S.col0, nx, ((long long)q * ny + y + dy) * nx, noisy, ok);
   };
@@ -408,7 +409,7 @@ __device__ __forceinline__ void first3_march(const StepArgs &a, const SlotDesc &
     const float2 zm = f2(float((q == 0) + (q == nz - 1)));
     const F4 miss = F4{add2(miss0.a, zm), add2(miss0.b, zm)};
     const F4 z = f4_mul(lap6(Xm, Xo, Xp, Xu, Xd, lft, rgt, miss), OPx);
-    if (S.io && (SQ == 1 || !a.v0_u)) f4_store(pV + (long long)q * PS, Xo);
+    if (S.io && (SQ >= 1 || !a.v0_u)) f4_store(pV + (long long)q * PS, Xo);
     q1 = fma2(z.a, Xo.a, fma2(z.b, Xo.b, q1));
     q3 = fma2(z.a, z.a, fma2(z.b, z.b, q3));
     q4 = fma2(Xo.a, Xo.a, fma2(Xo.b, Xo.b, q4));
@@ -503,7 +504,11 @@ static __global__ void __launch_bounds__(32 * BY3, 1) k3_first_f32(StepArgs a) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const uint32_t cell = (uint32_t)__cvta_generic_to_shared(ring3f + (size_t)w * RF3 * FRP3 + lane * 16);
   if (y < ny) {  // warp-uniform
+    // SQ 2: the sinc sequence with the polynomial force and no noise (the KG
+    // case), whose march holds only that arithmetic
     if (sq == 0) first3_march<0>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc, cell);
+    else if (s.nl_kind == NL_POLY && s.rm == 0.0 && s.r0 == 0.0)
+      first3_march<2>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc, cell);
     else first3_march<1>(a, s, S, y, t.p0, t.p1, step, OPx, miss0, acc, cell);
   }
   const bool keep = y < ny && S.io;
