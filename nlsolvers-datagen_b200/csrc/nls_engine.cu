@@ -692,8 +692,11 @@ int rebuild_tables(nls_pool *P) {
     max_ring = std::max(max_ring, h.ring_cnt);
     if (d.has_c) P->step_hc = 1;
   }
+  // ghost-ring blocks per slot: one point per thread, so the copies of a slot's
+  // ring take one memory round trip instead of one per point of a thread's
+  // grid-stride loop
   int rb = 1;
-  while (rb * 256 * 4 < max_ring && rb < 256) rb *= 2;
+  while (rb * 256 < max_ring && rb < 256) rb *= 2;
   P->ring_blocks = rb;
   for (TileSet *T : {&P->main, &P->main2, &P->first}) {
     T->live = (int)T->tiles.size();
