@@ -502,9 +502,10 @@ def other_configs_leg(steps=20, reps=3):
         shared_vel = None if dim == 2 else nl.pinned_empty((sp0.ns,) + sp0.shape)
         cases = [base[i % distinct] for i in range(B)]
         pts = ((n + 31) // 32 * 32) * n * (n if dim == 3 else 1)
-        # NLSE 2-D: 25-row pass segments, 12-row final tiles; 3-D: 88-plane segments (the default)
+        # NLSE 2-D: 25-row pass segments, 20-row final tiles (12 / 16 / 20 / 25 rows measured 0.537 /
+        # 0.543 / 0.534 / 0.570 ms per step); 3-D: 88-plane segments (the default)
         pool = Pool(method, dim, k, FP32, capacity_points=B * (pts + 256), max_slots=B,
-                    segment=25 if dim == 2 else None, final_segment=12 if dim == 2 else None)
+                    segment=25 if dim == 2 else None, final_segment=20 if dim == 2 else None)
         for cs in cases:
             assert pool.admit(*cs, traj=shared_traj, vel=shared_vel) is not None
         pool.step(3)
