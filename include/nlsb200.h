@@ -245,6 +245,12 @@ int nls_pool_sync(nls_pool *pool);
    place of nls_pool_sync. */
 int nls_pool_fence(nls_pool *pool, int32_t *ticket);
 int nls_pool_fence_wait(nls_pool *pool, int32_t ticket);
+/* Step the pool on streams of the device's greatest scheduling priority
+   (high != 0) or its least (high == 0, the default). Waits for the work queued
+   on the step's streams, then replaces them; call it between steps. When pools
+   share a GPU, the blocks of a high-priority pool's kernels are dispatched
+   before those of the others as SMs free up. */
+int nls_pool_set_priority(nls_pool *pool, int32_t high);
 /* Number of occupied slots, and free device points. */
 int nls_pool_usage(nls_pool *pool, int32_t *occupied, int64_t *free_points);
 /* 1: capture each step as a CUDA graph (default), 0: direct launches. */

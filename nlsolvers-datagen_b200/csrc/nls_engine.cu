@@ -2048,6 +2048,28 @@ int nls_pool_fence_wait(nls_pool *P, int32_t ticket) {
   return pool_status(P);
 }
 
+int nls_pool_set_priority(nls_pool *P, int32_t high) {
+  if (!P) return fail(NLS_ERR_INVALID_ARG, "null pool");
+  int least = 0, greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  const int prio = high ? greatest : least;
+  // the step's streams are replaced once the work queued on them is done;
+  // graphs and events are not bound to a stream and stay valid
+  CK(cudaStreamSynchronize(P->stream));
+  CK(cudaStreamSynchronize(P->stream2));
+  cudaStream_t s1 = nullptr, s2 = nullptr;
+  CK(cudaStreamCreateWithPriority(&s1, cudaStreamNonBlocking, prio));
+  if (cudaStreamCreateWithPriority(&s2, cudaStreamNonBlocking, prio) != cudaSuccess) {
+    cudaStreamDestroy(s1);
+    return fail(NLS_ERR_CUDA, "stream");
+  }
+  cudaStreamDestroy(P->stream);
+  cudaStreamDestroy(P->stream2);
+  P->stream = s1;
+  P->stream2 = s2;
+  return NLS_OK;
+}
+
 // device-side status of the slots (eigensolver convergence, divergence, waits)
 static int pool_status(nls_pool *P) {
   std::vector<SlotState> st(P->max_slots);

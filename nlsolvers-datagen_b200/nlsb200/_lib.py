@@ -37,7 +37,7 @@ SYMBOLS = [
     "nls_gautschi_step_noalloc", "nls_pool_set_diagnostics", "nls_set_diagnostics",
     "nls_pool_set_downsample", "nls_downsample_linear", "nls_pool_snapshots_ready",
     "nls_pool_set_downsample_fft", "nls_downsample_fft", "nls_pool_set_step_kernel", "nls_pool_set_wait_limit",
-    "nls_field2d", "nls_pool_fence", "nls_pool_fence_wait",
+    "nls_field2d", "nls_pool_fence", "nls_pool_fence_wait", "nls_pool_set_priority",
 ]
 
 
@@ -124,6 +124,7 @@ def lib() -> ctypes.CDLL:
         "nls_field2d": [i32, i32, ctypes.c_double, dp, i32, dp, i32, dp],
         "nls_pool_fence": [vp, ip],
         "nls_pool_fence_wait": [vp, i32],
+        "nls_pool_set_priority": [vp, i32],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

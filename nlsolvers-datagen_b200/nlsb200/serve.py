@@ -98,6 +98,7 @@ class PoolClass:
     precision: int = FP32
     max_slots: int = 32
     capacity_points: int | None = None  # None: the whole memory budget in this class's points
+    high_priority: bool = False  # step on the device's greatest stream priority (a latency class)
 
     @property
     def bytes_per_point(self) -> int:
@@ -138,7 +139,10 @@ class Server:
 
         def default_pool(pc):
             cap = pc.capacity_points or max(self.budget // pc.bytes_per_point, 1 << 16)
-            return Pool(pc.method, pc.dim, pc.k, pc.precision, cap, pc.max_slots)
+            pool = Pool(pc.method, pc.dim, pc.k, pc.precision, cap, pc.max_slots)
+            if pc.high_priority:
+                pool.set_priority(True)
+            return pool
         make_pool = make_pool or default_pool
         self.pools = {name: make_pool(pc) for name, pc in classes.items()}
 

@@ -412,6 +412,11 @@ class Pool:
         slot's device-side failure as sync() does."""
         check(lib().nls_pool_fence_wait(self._p, ticket))
 
+    def set_priority(self, high: bool):
+        """Step on streams of the device's greatest (True) or least (False,
+        the default) scheduling priority; waits for queued steps first."""
+        check(lib().nls_pool_set_priority(self._p, 1 if high else 0))
+
     def time_passes(self, j0: int, j1: int, reps: int):
         """Mean duration (ms) of one Lanczos pass launch over passes j0..j1
         launched back to back as the step issues them, and the grid points

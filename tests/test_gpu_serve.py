@@ -78,6 +78,46 @@ def test_pool_fences():
     pool.close()
 
 
+def test_priority_pools_keep_results():
+    """nls_pool_set_priority replaces the step's streams between steps (here
+    once before the first step and once in the middle of a run); a stream
+    served with one high-priority class equals its runs alone bitwise."""
+    import nlsb200 as nl
+    from nlsb200 import serve
+    from nlsb200 import workloads as W
+    sp, u0, v0, m, c = W.kg_case(64, 10.0, T=0.3, nt=30, ns=3, k=10, seed=4, precision=nl.FP32)
+    res = []
+    for switch in (False, True):
+        pool = nl.Pool(nl.KG_GAUTSCHI, 2, 10, nl.FP32, capacity_points=1 << 16, max_slots=1)
+        if switch:
+            pool.set_priority(True)
+        slot = pool.admit(sp, u0, v0, m)
+        pool.step(12)
+        if switch:
+            pool.set_priority(False)
+        pool.step(40)
+        pool.sync()
+        assert pool.poll(slot)[1]
+        res.append(pool.release(slot).traj)
+        pool.close()
+    assert np.array_equal(res[0], res[1])
+    reqs = serve.mixed_requests(10, rate_hz=300.0, seed=13, steps=(20, 50), scale=0.25, ns=3)
+    classes = serve.default_classes(reqs, max_slots=8)
+    name = sorted(classes)[0]
+    classes[name].high_priority = True
+    srv = serve.Server(classes, chunk=6, memory_budget=1 << 30)
+    st = srv.run(reqs, timeout_s=300)
+    srv.close()
+    assert st.completed == len(reqs)
+    for r in reqs:
+        if r.cls != name:
+            continue
+        with nl.Solver(r.spec, r.u0, r.v0, r.m, r.c) as sol:
+            sol.run()
+            traj, _ = sol.snapshots()
+        assert np.array_equal(traj, r.traj), r.cls
+
+
 def test_rank_share_of_a_placed_stream():
     """serve_rank on one GPU: the share of rank 0 of a stream placed over two
     GPUs completes, and its results equal solo runs bitwise (each GPU of a
